@@ -1,0 +1,205 @@
+"""ctypes access to the CPU oracle and to the host build of the reference.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` as the checker.  The product never
+imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libsphere_ref.so")
+REF_SRC_DEFAULT = "/root/reference/src"
+
+_FIELD4 = {"x", "vel", "angvel", "angpos", "force", "torque", "acc", "angacc",
+           "xyzsum", "walls_nx", "walls_mvfd", "bonds_delta", "bonds_omega"}
+_SLOT4 = {"delta_t", "distmod"}
+_U32 = {"cellid", "index", "cellstart", "cellend", "contacts", "bonds"}
+
+
+def build(ref: bool = True) -> None:
+    """Compile liboracle.so and, when the reference sources exist, _ref."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
+    ref_dir = os.environ.get("REF_DIR", REF_SRC_DEFAULT)
+    if ref and os.path.isdir(ref_dir):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_DIR={ref_dir}"])
+
+
+def _load(path):
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built (run oracle.build())")
+    return ctypes.CDLL(path)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = _load(ORACLE_SO)
+        _lib.orc_load.restype = ctypes.c_void_p
+        _lib.orc_load.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_int)]
+        _lib.orc_free.argtypes = [ctypes.c_void_p]
+        _lib.orc_step.argtypes = [ctypes.c_void_p, ctypes.c_int64]
+        _lib.orc_step.restype = ctypes.c_int
+        _lib.orc_error.argtypes = [ctypes.c_void_p]
+        _lib.orc_error.restype = ctypes.c_char_p
+        _lib.orc_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p,
+                                 ctypes.c_void_p, ctypes.c_size_t]
+        _lib.orc_get.restype = ctypes.c_int64
+        _lib.orc_set.argtypes = [ctypes.c_void_p, ctypes.c_char_p,
+                                 ctypes.c_void_p, ctypes.c_size_t]
+        _lib.orc_write_bin.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        for f in ("orc_np", "orc_nc", "orc_nw"):
+            getattr(_lib, f).argtypes = [ctypes.c_void_p]
+        for f in ("orc_stage_hash_sort_reorder", "orc_stage_topology",
+                  "orc_stage_interact"):
+            getattr(_lib, f).argtypes = [ctypes.c_void_p]
+            getattr(_lib, f).restype = ctypes.c_int
+    return _lib
+
+
+def _shape(name, nbytes):
+    if name in _FIELD4:
+        return numpy.float64, (nbytes // 32, 4)
+    if name in _SLOT4:
+        return numpy.float64, (nbytes // 32, 4)
+    if name in _U32:
+        return numpy.uint32, (nbytes // 4,)
+    if name in ("iter", "darcy_nijac_last", "darcy_nijac_total"):
+        return numpy.int64, (nbytes // 8,)
+    if name == "darcy_p_constant":
+        return numpy.int32, (nbytes // 4,)
+    return numpy.float64, (nbytes // 8,)
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+class Oracle:
+    """The CPU oracle's state for one ``.bin`` input."""
+
+    def __init__(self, path, fluid=False, precision="faithful", integrator=3, nc=32):
+        status = ctypes.c_int(0)
+        prec = {"faithful": 0, "fp64": 1, "true": 1}[precision]
+        self._h = lib().orc_load(os.fsencode(path), int(bool(fluid)), prec,
+                                 int(integrator), int(nc), ctypes.byref(status))
+        if not self._h:
+            raise OracleError(f"orc_load failed with status {status.value}")
+
+    def close(self):
+        if self._h:
+            lib().orc_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n=1):
+        rc = lib().orc_step(self._h, int(n))
+        return rc
+
+    def error(self):
+        return lib().orc_error(self._h).decode()
+
+    def get(self, name):
+        need = lib().orc_get(self._h, name.encode(), None, 0)
+        if need < 0:
+            raise KeyError(name)
+        dtype, shape = _shape(name, need)
+        out = numpy.empty(shape, dtype=dtype)
+        rc = lib().orc_get(self._h, name.encode(), out.ctypes.data, out.nbytes)
+        if rc != 0:
+            raise OracleError(f"orc_get({name}) returned {rc}")
+        return out
+
+    def set(self, name, arr):
+        arr = numpy.ascontiguousarray(arr)
+        rc = lib().orc_set(self._h, name.encode(), arr.ctypes.data, arr.nbytes)
+        if rc != 0:
+            raise OracleError(f"orc_set({name}) returned {rc}")
+
+    def stage(self, which):
+        fn = {"sort": lib().orc_stage_hash_sort_reorder,
+              "topology": lib().orc_stage_topology,
+              "interact": lib().orc_stage_interact}[which]
+        return fn(self._h)
+
+    def write_bin(self, path):
+        return lib().orc_write_bin(self._h, os.fsencode(path))
+
+    @property
+    def np(self):
+        return lib().orc_np(self._h)
+
+    @property
+    def nc(self):
+        return lib().orc_nc(self._h)
+
+
+_ref = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        _ref = _load(REF_SO)
+        _ref.ref_open.restype = ctypes.c_void_p
+        _ref.ref_open.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        _ref.ref_step.argtypes = [ctypes.c_void_p, ctypes.c_long]
+        _ref.ref_write.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        _ref.ref_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p,
+                                 ctypes.c_void_p, ctypes.c_size_t]
+        _ref.ref_get.restype = ctypes.c_long
+        _ref.ref_close.argtypes = [ctypes.c_void_p]
+    return _ref
+
+
+class Reference:
+    """The reference's own kernels compiled for the host (oracle/_ref)."""
+
+    def __init__(self, path, fluid=False):
+        self._h = ref_lib().ref_open(os.fsencode(path), int(bool(fluid)))
+
+    def step(self, n=1):
+        return ref_lib().ref_step(self._h, int(n))
+
+    def get(self, name):
+        need = ref_lib().ref_get(self._h, name.encode(), None, 0)
+        if need < 0:
+            raise KeyError(name)
+        dtype, shape = _shape(name, need)
+        out = numpy.empty(shape, dtype=dtype)
+        ref_lib().ref_get(self._h, name.encode(), out.ctypes.data, out.nbytes)
+        return out
+
+    def write_bin(self, path):
+        return ref_lib().ref_write(self._h, os.fsencode(path))
+
+    def close(self):
+        if self._h:
+            ref_lib().ref_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

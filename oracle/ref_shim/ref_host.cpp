@@ -1,0 +1,371 @@
+/*
+ * Host build of the reference's own DEM step -- TEST INFRASTRUCTURE ONLY.
+ *
+ * The reference kernels (sorting.cuh, contactmodels.cuh, cohesion.cuh,
+ * contactsearch.cuh, integration.cuh) are #included unchanged from the
+ * reference tree (REF_DIR) and run one thread at a time through a serial
+ * launch loop.  The reference's own DEM constructor, readbin/writebin and
+ * checkValues (sphere.cpp, file_io.cpp) are linked unchanged; this file
+ * supplies host versions of the device-memory members of device.cu and a
+ * step driver that follows the stage order of DEM::startTime
+ * (device.cu:1038-2550).  The result is the reference run here, used to pin
+ * the C oracle.  Thrust's stable sort_by_key is replaced by std::stable_sort
+ * of (key, index) pairs, which yields the same permutation.
+ */
+#include "ref_shim.h"
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdlib>
+#include <string>
+#include <vector>
+
+#define private public
+#include "sphere.h"
+#undef private
+#include "datatypes.h"
+#include "constants.cuh"
+#include "vector_arithmetic.h"
+
+uint3 ref_threadIdx, ref_blockIdx;
+dim3 ref_blockDim, ref_gridDim;
+/* backing store for `extern __shared__` arrays (reorderArrays) */
+unsigned int shared_data[1025];
+
+#include "sorting.cuh"
+#include "contactmodels.cuh"
+#include "cohesion.cuh"
+#include "contactsearch.cuh"
+#include "integration.cuh"
+
+template <class F> static void launch(unsigned grid, unsigned block, F f)
+{
+    ref_gridDim = dim3(grid, 1, 1);
+    ref_blockDim = dim3(block, 1, 1);
+    for (unsigned b = 0; b < grid; ++b) {
+        ref_blockIdx = make_uint3(b, 0, 0);
+        for (unsigned t = 0; t < block; ++t) {
+            ref_threadIdx = make_uint3(t, 0, 0);
+            f();
+        }
+    }
+}
+
+static unsigned idiv_up(unsigned a, unsigned b) { return (a % b != 0) ? (a / b + 1) : (a / b); }
+
+/* ---- host stand-ins for the device-memory members of device.cu ---- */
+void DEM::initializeGPU() {}
+void DEM::checkForCudaErrors(const char *, const int) {}
+void DEM::checkForCudaErrorsIter(const char *, const unsigned int, const int) {}
+void DEM::transferToConstantDeviceMemory()
+{
+    /* device.cu:331-357 */
+    devC_nd = nd;
+    devC_np = np;
+    devC_nw = walls.nw;
+    devC_nc = NC;
+    devC_dt = time.dt;
+    devC_nb0 = params.nb0;
+    devC_params = params;
+    devC_grid = grid;
+}
+
+template <class T> static T *halloc(size_t n)
+{
+    T *p = new T[n ? n : 1];
+    std::memset((void *)p, 0, sizeof(T) * (n ? n : 1));
+    return p;
+}
+
+void DEM::allocateGlobalDeviceMemory()
+{
+    /* device.cu:405-487; the history arrays start at zero (the reference
+     * copies uninitialised host memory). */
+    k.acc = halloc<Float4>(np);
+    k.angacc = halloc<Float4>(np);
+    dev_x = halloc<Float4>(np); dev_xyzsum = halloc<Float4>(np);
+    dev_vel = halloc<Float4>(np); dev_vel0 = halloc<Float4>(np);
+    dev_acc = halloc<Float4>(np); dev_force = halloc<Float4>(np);
+    dev_angpos = halloc<Float4>(np); dev_angvel = halloc<Float4>(np);
+    dev_angvel0 = halloc<Float4>(np); dev_angacc = halloc<Float4>(np);
+    dev_torque = halloc<Float4>(np);
+    dev_contacts = halloc<unsigned int>((size_t)np * NC);
+    dev_distmod = halloc<Float4>((size_t)np * NC);
+    dev_delta_t = halloc<Float4>((size_t)np * NC);
+    dev_bonds = halloc<uint2>(params.nb0);
+    dev_bonds_delta = halloc<Float4>(params.nb0);
+    dev_bonds_omega = halloc<Float4>(params.nb0);
+    dev_x_sorted = halloc<Float4>(np); dev_vel_sorted = halloc<Float4>(np);
+    dev_angvel_sorted = halloc<Float4>(np);
+    dev_es_dot = halloc<Float>(np); dev_es = halloc<Float>(np);
+    dev_ev_dot = halloc<Float>(np); dev_ev = halloc<Float>(np);
+    dev_p = halloc<Float>(np);
+    dev_gridParticleCellID = halloc<unsigned int>(np);
+    dev_gridParticleIndex = halloc<unsigned int>(np);
+    size_t ncell = (size_t)grid.num[0] * grid.num[1] * grid.num[2];
+    dev_cellStart = halloc<unsigned int>(ncell);
+    dev_cellEnd = halloc<unsigned int>(ncell);
+    k.contacts = halloc<unsigned int>((size_t)np * NC);
+    for (size_t i = 0; i < (size_t)np * NC; ++i) k.contacts[i] = np;
+    k.distmod = halloc<Float4>((size_t)np * NC);
+    k.delta_t = halloc<Float4>((size_t)np * NC);
+    unsigned nw = walls.nw;
+    dev_walls_wmode = halloc<int>(nw);
+    dev_walls_nx = halloc<Float4>(nw);
+    dev_walls_mvfd = halloc<Float4>(nw);
+    dev_walls_tau_x = halloc<Float>(nw);
+    dev_walls_tau_eff_x_pp = halloc<Float>((size_t)nw * np);
+    dev_walls_force_pp = halloc<Float>((size_t)nw * np);
+    dev_walls_acc = halloc<Float>(nw);
+    unsigned blocks = idiv_up(np, 256);
+    dev_walls_force_partial = halloc<Float>((size_t)blocks * (nw ? nw : 1));
+    dev_walls_tau_eff_x_partial = halloc<Float>((size_t)blocks * (nw ? nw : 1));
+}
+
+void DEM::transferToGlobalDeviceMemory(int)
+{
+    /* device.cu:667-752 */
+    size_t f4 = sizeof(Float4) * np, f1 = sizeof(Float) * np;
+    std::memcpy(dev_x, k.x, f4); std::memcpy(dev_xyzsum, k.xyzsum, f4);
+    std::memcpy(dev_vel, k.vel, f4); std::memcpy(dev_vel0, k.vel, f4);
+    std::memcpy(dev_acc, k.acc, f4); std::memcpy(dev_force, k.force, f4);
+    std::memcpy(dev_angpos, k.angpos, f4); std::memcpy(dev_angvel, k.angvel, f4);
+    std::memcpy(dev_angvel0, k.angvel, f4); std::memcpy(dev_angacc, k.angacc, f4);
+    std::memcpy(dev_torque, k.torque, f4);
+    std::memcpy(dev_contacts, k.contacts, sizeof(unsigned int) * np * NC);
+    std::memcpy(dev_distmod, k.distmod, f4 * NC);
+    std::memcpy(dev_delta_t, k.delta_t, f4 * NC);
+    if (params.nb0) {
+        std::memcpy(dev_bonds, k.bonds, sizeof(uint2) * params.nb0);
+        std::memcpy(dev_bonds_delta, k.bonds_delta, sizeof(Float4) * params.nb0);
+        std::memcpy(dev_bonds_omega, k.bonds_omega, sizeof(Float4) * params.nb0);
+    }
+    std::memcpy(dev_es_dot, e.es_dot, f1); std::memcpy(dev_es, e.es, f1);
+    std::memcpy(dev_ev_dot, e.ev_dot, f1); std::memcpy(dev_ev, e.ev, f1);
+    std::memcpy(dev_p, e.p, f1);
+    std::memcpy(dev_walls_wmode, walls.wmode, sizeof(int) * walls.nw);
+    std::memcpy(dev_walls_nx, walls.nx, sizeof(Float4) * walls.nw);
+    std::memcpy(dev_walls_mvfd, walls.mvfd, sizeof(Float4) * walls.nw);
+    if (walls.nw) std::memcpy(dev_walls_tau_x, walls.tau_x, sizeof(Float));
+}
+
+void DEM::transferFromGlobalDeviceMemory()
+{
+    /* device.cu:754-829 */
+    size_t f4 = sizeof(Float4) * np, f1 = sizeof(Float) * np;
+    std::memcpy(k.x, dev_x, f4); std::memcpy(k.xyzsum, dev_xyzsum, f4);
+    std::memcpy(k.vel, dev_vel, f4); std::memcpy(k.acc, dev_acc, f4);
+    std::memcpy(k.force, dev_force, f4); std::memcpy(k.angpos, dev_angpos, f4);
+    std::memcpy(k.angvel, dev_angvel, f4); std::memcpy(k.angacc, dev_angacc, f4);
+    std::memcpy(k.torque, dev_torque, f4);
+    std::memcpy(k.contacts, dev_contacts, sizeof(unsigned int) * np * NC);
+    std::memcpy(k.distmod, dev_distmod, f4 * NC);
+    std::memcpy(k.delta_t, dev_delta_t, f4 * NC);
+    if (params.nb0) {
+        std::memcpy(k.bonds, dev_bonds, sizeof(uint2) * params.nb0);
+        std::memcpy(k.bonds_delta, dev_bonds_delta, sizeof(Float4) * params.nb0);
+        std::memcpy(k.bonds_omega, dev_bonds_omega, sizeof(Float4) * params.nb0);
+    }
+    std::memcpy(e.es_dot, dev_es_dot, f1); std::memcpy(e.es, dev_es, f1);
+    std::memcpy(e.ev_dot, dev_ev_dot, f1); std::memcpy(e.ev, dev_ev, f1);
+    std::memcpy(e.p, dev_p, f1);
+    std::memcpy(walls.nx, dev_walls_nx, sizeof(Float4) * walls.nw);
+    std::memcpy(walls.mvfd, dev_walls_mvfd, sizeof(Float4) * walls.nw);
+}
+
+void DEM::freeGlobalDeviceMemory() {}
+void DEM::initDarcyMemDev() { std::fprintf(stderr, "reference host build: Darcy not wired\n"); std::abort(); }
+
+/* ---- the step driver: DEM::startTime's loop body, dry part ---- */
+struct RefRun {
+    DEM *dem;
+    long iter;
+    int velocity_state;
+};
+
+/* summation (integration.cuh:309-341) uses a 256-wide shared-memory tree
+ * across the threads of a block; that cannot run one thread at a time, so
+ * it is restated here with the same order of additions. */
+static void ref_summation(const Float *in, Float *out, unsigned np, unsigned blocks)
+{
+    Float cache[256];
+    for (unsigned b = 0; b < blocks; ++b) {
+        for (unsigned t = 0; t < 256; ++t) {
+            unsigned idx = t + b * 256;
+            Float temp = 0.0f;
+            while (idx < np) { temp += in[idx]; idx += 256 * blocks; }
+            cache[t] = temp;
+        }
+        for (unsigned i = 128; i != 0; i /= 2)
+            for (unsigned t = 0; t < i; ++t) cache[t] += cache[t + i];
+        out[b] = cache[0];
+    }
+}
+
+static int ref_one_step(RefRun *r)
+{
+    DEM &d = *r->dem;
+    unsigned np = d.np;
+    unsigned tpb = 256, bpg = idiv_up(np, tpb);
+    unsigned bpg_bonds = idiv_up(d.params.nb0, tpb);
+    if (np > 0) {
+        launch(bpg, tpb, [&] {
+            calcParticleCellID(d.dev_gridParticleCellID, d.dev_gridParticleIndex, d.dev_x);
+        });
+        /* thrust::sort_by_key (device.cu:1082-1085): stable */
+        std::vector<std::pair<unsigned, unsigned>> kv(np);
+        for (unsigned i = 0; i < np; ++i) kv[i] = {d.dev_gridParticleCellID[i], d.dev_gridParticleIndex[i]};
+        std::stable_sort(kv.begin(), kv.end(),
+                         [](const std::pair<unsigned, unsigned> &a,
+                            const std::pair<unsigned, unsigned> &b) { return a.first < b.first; });
+        for (unsigned i = 0; i < np; ++i) {
+            d.dev_gridParticleCellID[i] = kv[i].first;
+            d.dev_gridParticleIndex[i] = kv[i].second;
+        }
+        std::memset(d.dev_cellStart, 0xff,
+                    sizeof(unsigned) * d.grid.num[0] * d.grid.num[1] * d.grid.num[2]);
+        launch(bpg, tpb, [&] {
+            reorderArrays(d.dev_cellStart, d.dev_cellEnd, d.dev_gridParticleCellID,
+                          d.dev_gridParticleIndex, d.dev_x, d.dev_vel, d.dev_angvel,
+                          d.dev_x_sorted, d.dev_vel_sorted, d.dev_angvel_sorted);
+        });
+        if (d.params.contactmodel == 2 || d.params.contactmodel == 3) {
+            launch(bpg, tpb, [&] {
+                topology(d.dev_cellStart, d.dev_cellEnd, d.dev_gridParticleIndex,
+                         d.dev_x_sorted, d.dev_contacts, d.dev_distmod);
+            });
+        }
+        launch(bpg, tpb, [&] {
+            interact(d.dev_gridParticleIndex, d.dev_cellStart, d.dev_cellEnd, d.dev_x,
+                     d.dev_x_sorted, d.dev_vel_sorted, d.dev_angvel_sorted, d.dev_vel,
+                     d.dev_angvel, d.dev_force, d.dev_torque, d.dev_es_dot,
+                     d.dev_ev_dot, d.dev_es, d.dev_ev, d.dev_p, d.dev_walls_nx,
+                     d.dev_walls_mvfd, d.dev_walls_force_pp, d.dev_contacts,
+                     d.dev_distmod, d.dev_delta_t);
+        });
+        if (d.params.nb0 > 0) {
+            launch(bpg_bonds, tpb, [&] {
+                bondsLinear(d.dev_bonds, d.dev_bonds_delta, d.dev_bonds_omega, d.dev_x,
+                            d.dev_vel, d.dev_angvel, d.dev_force, d.dev_torque);
+            });
+        }
+    }
+    if (np > 0) {
+        if (d.walls.nw > 0 && d.walls.wmode[0] == 3) {
+            launch(bpg, tpb, [&] {
+                findShearStressOnFixedMovingParticles(d.dev_x, d.dev_vel, d.dev_force,
+                                                      d.dev_walls_tau_eff_x_pp);
+            });
+            ref_summation(d.dev_walls_tau_eff_x_pp, d.dev_walls_tau_eff_x_partial, np, bpg);
+        }
+        int change_velocity_state = 0;
+        const Float velocity_factor = 10.0, v2_start = 10.0, v2_end = 15.0;
+        if (d.time.current >= v2_start && d.time.current < v2_end && r->velocity_state == 1) {
+            change_velocity_state = 1;
+            r->velocity_state = 2;
+        } else if (d.time.current >= v2_end && r->velocity_state == 2) {
+            change_velocity_state = -1;
+            r->velocity_state = 1;
+        }
+        launch(bpg, tpb, [&] {
+            integrate(d.dev_x_sorted, d.dev_vel_sorted, d.dev_angvel_sorted, d.dev_x,
+                      d.dev_vel, d.dev_angvel, d.dev_force, d.dev_torque, d.dev_angpos,
+                      d.dev_acc, d.dev_angacc, d.dev_vel0, d.dev_angvel0, d.dev_xyzsum,
+                      d.dev_gridParticleIndex, (unsigned)r->iter, d.dev_walls_wmode,
+                      d.dev_walls_mvfd, d.dev_walls_tau_eff_x_partial,
+                      d.dev_walls_tau_x, d.walls.nw ? d.walls.tau_x[0] : 0.0,
+                      change_velocity_state, velocity_factor, bpg);
+        });
+        if (d.walls.nw > 0) {
+            ref_summation(d.dev_walls_force_pp, d.dev_walls_force_partial, np, bpg);
+            launch(1, d.walls.nw, [&] {
+                integrateWalls(d.dev_walls_nx, d.dev_walls_mvfd, d.dev_walls_wmode,
+                               d.dev_walls_force_partial, d.dev_walls_acc, bpg,
+                               d.time.current, (unsigned)r->iter);
+            });
+        }
+    }
+    d.time.current += d.time.dt;
+    ++r->iter;
+    return 0;
+}
+
+extern "C" {
+
+void *ref_open(const char *path, int fluid)
+{
+    /* DEM(inputbin, verbosity, checkVals, dry, initCuda, transferConstMem,
+     *     fluidFlow, device) -- sphere.h */
+    DEM *d = new DEM(std::string(path), 0, 1, 0, 1, 1, fluid, 0);
+    RefRun *r = new RefRun{d, 0, 1};
+    return r;
+}
+
+int ref_step(void *h, long n)
+{
+    RefRun *r = (RefRun *)h;
+    for (long i = 0; i < n; ++i) {
+        r->dem->transferToConstantDeviceMemory();
+        int rc = ref_one_step(r);
+        if (rc) return rc;
+    }
+    r->dem->transferFromGlobalDeviceMemory();
+    return 0;
+}
+
+int ref_write(void *h, const char *path)
+{
+    RefRun *r = (RefRun *)h;
+    r->dem->transferFromGlobalDeviceMemory();
+    r->dem->writebin(path);
+    return 0;
+}
+
+long ref_get(void *h, const char *name, void *dst, size_t bytes)
+{
+    RefRun *r = (RefRun *)h;
+    DEM &d = *r->dem;
+    const void *src = nullptr;
+    size_t need = 0;
+    size_t np = d.np, slots = (size_t)d.np * NC;
+    std::string n(name);
+    if (n == "x") { src = d.dev_x; need = np * 32; }
+    else if (n == "vel") { src = d.dev_vel; need = np * 32; }
+    else if (n == "angvel") { src = d.dev_angvel; need = np * 32; }
+    else if (n == "angpos") { src = d.dev_angpos; need = np * 32; }
+    else if (n == "force") { src = d.dev_force; need = np * 32; }
+    else if (n == "torque") { src = d.dev_torque; need = np * 32; }
+    else if (n == "acc") { src = d.dev_acc; need = np * 32; }
+    else if (n == "angacc") { src = d.dev_angacc; need = np * 32; }
+    else if (n == "xyzsum") { src = d.dev_xyzsum; need = np * 32; }
+    else if (n == "es_dot") { src = d.dev_es_dot; need = np * 8; }
+    else if (n == "es") { src = d.dev_es; need = np * 8; }
+    else if (n == "ev_dot") { src = d.dev_ev_dot; need = np * 8; }
+    else if (n == "ev") { src = d.dev_ev; need = np * 8; }
+    else if (n == "p") { src = d.dev_p; need = np * 8; }
+    else if (n == "cellid") { src = d.dev_gridParticleCellID; need = np * 4; }
+    else if (n == "index") { src = d.dev_gridParticleIndex; need = np * 4; }
+    else if (n == "contacts") { src = d.dev_contacts; need = slots * 4; }
+    else if (n == "delta_t") { src = d.dev_delta_t; need = slots * 32; }
+    else if (n == "distmod") { src = d.dev_distmod; need = slots * 32; }
+    else if (n == "walls_nx") { src = d.dev_walls_nx; need = d.walls.nw * 32; }
+    else if (n == "walls_mvfd") { src = d.dev_walls_mvfd; need = d.walls.nw * 32; }
+    else if (n == "cellstart") {
+        src = d.dev_cellStart; need = 4 * (size_t)d.grid.num[0] * d.grid.num[1] * d.grid.num[2];
+    } else if (n == "bonds") { src = d.dev_bonds; need = 8 * (size_t)d.params.nb0; }
+    else if (n == "bonds_delta") { src = d.dev_bonds_delta; need = 32 * (size_t)d.params.nb0; }
+    else if (n == "bonds_omega") { src = d.dev_bonds_omega; need = 32 * (size_t)d.params.nb0; }
+    else return -1;
+    if (!dst || bytes < need) return (long)need;
+    std::memcpy(dst, src, need);
+    return 0;
+}
+
+void ref_close(void *h)
+{
+    RefRun *r = (RefRun *)h;
+    delete r->dem;
+    delete r;
+}
+
+}  /* extern "C" */

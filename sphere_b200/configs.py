@@ -1,0 +1,241 @@
+"""Seeded synthetic workloads for the DEM step.
+
+Each generator returns a :class:`~sphere_b200.binfile.BinData` built the way
+the reference's Python setup helpers would build it, so the same file can be
+run by this engine, the oracle and the reference.  Seeds are explicit; the
+same seed gives the same bytes.
+
+Workloads (the sizes of the published benchmark configurations):
+
+* :func:`settling_lattice` -- dry settling of N spheres on a cubic lattice
+  (N = 10,000, radii U(0.009, 0.011) m, spacing 0.025 m, jitter +/-0.002 m,
+  periodic x/y, linear contact k_n = k_t = 1.16e7 N/m, mu = 0.5).
+* :func:`shear_box` -- a dense packing under a top wall at normal stress
+  sigma0 with the top layer sheared along x (N = 100,000, radii
+  U(0.008, 0.012) m, Young's modulus contact E = 7e8 Pa, mu = 0.5).
+* :func:`two_particle` / :func:`wall_particle` -- the reference's collision
+  test set-ups (``tests/contactmodel.py``, ``tests/contactmodel_wall.py``).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy
+
+from .binfile import BinData
+
+
+def time_step(d: BinData, epsilon: float = 0.01) -> float:
+    """The reference's automatic time step (``python/sphere.py:3307-3376``):
+    dt = epsilon / sqrt(k_max / m_min)."""
+    r_min = numpy.min(d.radius)
+    m_min = d.rho * 4.0 / 3.0 * numpy.pi * r_min ** 3
+    if d.E > 0.001:
+        k_max = numpy.max(numpy.pi / 2.0 * d.E * d.radius)
+    else:
+        k_max = numpy.max([d.k_n, d.k_t])
+    return float(epsilon / (numpy.sqrt(k_max / m_min)))
+
+
+def init_temporal(d: BinData, total: float, file_dt: float = 0.05,
+                  current: float = 0.0, epsilon: float = 0.01) -> None:
+    d.time_dt = time_step(d, epsilon)
+    d.time_current = current
+    d.time_total = total
+    d.time_file_dt = file_dt
+    d.time_step_count = 0
+
+
+def _particles(d: BinData, n: int) -> None:
+    d.np = n
+    d.x = numpy.zeros((n, 3))
+    d.radius = numpy.ones(n)
+    d.xyzsum = numpy.zeros((n, 3))
+    d.vel = numpy.zeros((n, 3))
+    d.fixvel = numpy.zeros(n)
+    d.force = numpy.zeros((n, 3))
+    d.angpos = numpy.zeros((n, 3))
+    d.angvel = numpy.zeros((n, 3))
+    d.torque = numpy.zeros((n, 3))
+    d.es_dot = numpy.zeros(n)
+    d.es = numpy.zeros(n)
+    d.ev_dot = numpy.zeros(n)
+    d.ev = numpy.zeros(n)
+    d.p = numpy.zeros(n)
+    d.color = numpy.zeros(n, dtype=numpy.int32)
+
+
+def default_params(d: BinData, mu_s=0.5, mu_d=0.5, rho=2600.0, k_n=1.16e9,
+                   k_t=1.16e9, gamma_n=0.0, gamma_t=0.0, gamma_wn=1.0e4,
+                   gamma_wt=1.0e4) -> None:
+    """``sim.defaultParams`` (``python/sphere.py:3762-3858``) without
+    capillary cohesion."""
+    d.rho = rho
+    d.k_n = k_n
+    d.k_t = k_t
+    d.k_r = 0.0
+    d.gamma_n = gamma_n
+    d.gamma_t = gamma_t
+    d.gamma_r = 0.0
+    d.mu_s = mu_s
+    d.mu_d = mu_d
+    d.mu_r = 0.0
+    d.gamma_wn = gamma_wn
+    d.gamma_wt = gamma_wt
+    d.mu_ws = mu_s
+    d.mu_wd = mu_d
+    d.kappa = 0.0
+    d.V_b = 0.0
+    d.db = 0.0
+
+
+def grid_for(d: BinData, L, origo=(0.0, 0.0, 0.0), dx: float = -1.0) -> None:
+    """``sim.defineWorldBoundaries`` (``python/sphere.py:2607-2653``)."""
+    cell = dx if dx > 0.0 else 2.1 * numpy.amax(d.radius)
+    d.origo = numpy.asarray(origo, dtype=numpy.float64).copy()
+    d.L = numpy.asarray(L, dtype=numpy.float64).copy()
+    d.num = numpy.ceil((d.L - d.origo) / cell).astype(numpy.uint32)
+    if numpy.any(d.num < 3):
+        raise ValueError(f"grid must be at least 3 cells per axis, got {d.num}")
+
+
+def settling_lattice(n: int = 10000, seed: int = 0, nx: int = 22, ny: int = 22,
+                     nz: int = 21, spacing: float = 0.025, jitter: float = 0.002,
+                     r_min: float = 0.009, r_max: float = 0.011,
+                     steps: int = 20000, contactmodel: int = 2) -> BinData:
+    """Dry settling: N spheres on the first N sites of an nx*ny*nz cubic
+    lattice, seeded jitter, radii and velocities; periodic x/y, no dynamic
+    walls (the implicit bottom wall at origo.z and the fixed top at L.z
+    apply)."""
+    if n > nx * ny * nz:
+        raise ValueError("lattice too small for n particles")
+    rng = numpy.random.default_rng(seed)
+    d = BinData()
+    _particles(d, n)
+    idx = numpy.arange(n)
+    ix, iy, iz = idx % nx, (idx // nx) % ny, idx // (nx * ny)
+    centres = numpy.column_stack([ix, iy, iz]).astype(numpy.float64)
+    d.x = (centres + 0.5) * spacing + rng.uniform(-jitter, jitter, size=(n, 3))
+    d.radius = rng.uniform(r_min, r_max, size=n)
+    d.vel = rng.uniform(-0.01, 0.01, size=(n, 3))
+    default_params(d, mu_s=0.5, mu_d=0.5, k_n=1.16e7, k_t=1.16e7)
+    d.contactmodel = contactmodel
+    d.g = numpy.array([0.0, 0.0, -9.81])
+    side = max(nx, ny) * spacing
+    grid_for(d, L=[nx * spacing, ny * spacing, side])
+    d.periodic = 1
+    d.nw = 0
+    dt = time_step(d)
+    init_temporal(d, total=steps * dt, file_dt=steps * dt * 2.0)
+    return d
+
+
+def two_particle(radii=(1.0, 1.0), z=(2.0, 4.05), vel0=1.0, gamma_n=0.0,
+                 E=0.0, angle_x=0.0, mu=0.5, total=0.1, file_dt=0.01) -> BinData:
+    """The reference's two-particle collision set-up (``tests/contactmodel.py``):
+    particle 0 moves towards particle 1 along z, world 10 m cubed, no
+    gravity, sphere's default stiffness 1.16e9 N/m."""
+    d = BinData()
+    _particles(d, 2)
+    d.radius = numpy.asarray(radii, dtype=numpy.float64).copy()
+    d.x[0, :] = [5.0, 5.0, z[0]]
+    d.x[1, :] = [5.0 + angle_x, 5.0, z[1]]
+    d.vel[0, 2] = vel0
+    default_params(d, mu_s=mu, mu_d=mu, gamma_wn=1.0e3, gamma_wt=0.0)
+    d.gamma_n = gamma_n
+    d.E = E
+    grid_for(d, L=[10.0, 10.0, 10.0])
+    init_temporal(d, total=total, file_dt=file_dt)
+    return d
+
+
+def wall_particle(radius=1.0, z=1.05, vel0=-1.0, gamma_wn=0.0, E=0.0,
+                  total=0.1, file_dt=0.01) -> BinData:
+    """One particle moving into the implicit bottom wall
+    (``tests/contactmodel_wall.py``)."""
+    d = BinData()
+    _particles(d, 1)
+    d.radius[:] = radius
+    d.x[0, :] = [5.0, 5.0, z]
+    d.vel[0, 2] = vel0
+    default_params(d, gamma_wn=gamma_wn, gamma_wt=0.0)
+    d.E = E
+    grid_for(d, L=[10.0, 10.0, 10.0])
+    init_temporal(d, total=total, file_dt=file_dt)
+    return d
+
+
+def random_packing(n: int, seed: int, r_min: float, r_max: float,
+                   fill: float = 0.9, width_cells: int = 0) -> BinData:
+    """Jittered close-spaced lattice of n spheres (no overlaps), a cheap
+    stand-in for a settled packing: spacing 2*r_max*(1+gap), seeded radii."""
+    rng = numpy.random.default_rng(seed)
+    d = BinData()
+    _particles(d, n)
+    spacing = 2.0 * r_max * 1.002
+    side = int(math.ceil(math.sqrt(n / 1.0) ** (2.0 / 3.0))) if width_cells <= 0 else width_cells
+    side = max(side, 3)
+    nz = int(math.ceil(n / (side * side)))
+    idx = numpy.arange(n)
+    ix, iy, iz = idx % side, (idx // side) % side, idx // (side * side)
+    centres = numpy.column_stack([ix, iy, iz]).astype(numpy.float64)
+    jit = 0.001 * r_max
+    d.x = (centres + 0.5) * spacing + rng.uniform(-jit, jit, size=(n, 3))
+    d.radius = rng.uniform(r_min, r_max, size=n)
+    default_params(d, mu_s=0.5, mu_d=0.5, k_n=1.16e7, k_t=1.16e7)
+    d.g = numpy.array([0.0, 0.0, -9.81])
+    cell = 2.1 * r_max
+    Lxy = side * spacing
+    grid_for(d, L=[Lxy, Lxy, (nz + 2) * spacing], dx=Lxy / max(3, int(Lxy // cell)))
+    d.periodic = 1
+    _ = fill
+    return d
+
+
+def add_top_wall(d: BinData, sigma0: float, wmode: int = 1, mass=None) -> None:
+    """One dynamic top wall at the highest particle surface
+    (``sim.adjustUpperWall`` + ``consolidate``, ``python/sphere.py:2949-3048``)."""
+    zmax = float(numpy.max(d.x[:, 2] + d.radius))
+    d.nw = 1
+    d.wmode = numpy.array([wmode], dtype=numpy.int32)
+    d.w_n = numpy.array([[0.0, 0.0, -1.0]])
+    d.w_x = numpy.array([zmax])
+    m = float(numpy.sum(d.rho * 4.0 / 3.0 * numpy.pi * d.radius ** 3)) if mass is None else mass
+    d.w_m = numpy.array([m])
+    d.w_vel = numpy.zeros(1)
+    d.w_force = numpy.zeros(1)
+    d.w_sigma0 = numpy.array([sigma0])
+
+
+def shear_setup(d: BinData, shear_velocity: float, sigma0: float) -> None:
+    """``sim.shear`` (``python/sphere.py:3097-3165``) at a given top-layer
+    velocity: bottom and top layers get fixvel = 1, the top layer moves at
+    shear_velocity along x, one stress-controlled top wall, no wall friction."""
+    z_min = numpy.min(d.x[:, 2] - d.radius)
+    z_max = numpy.max(d.x[:, 2] + d.radius)
+    cell = d.L[0] / d.num[0]
+    d.num = d.num.copy()
+    d.num[2] += 1
+    d.L = d.L.copy()
+    d.L[2] = d.num[2] * cell
+    d.vel[:] = 0.0
+    d.angvel[:] = 0.0
+    d.force[:] = 0.0
+    d.torque[:] = 0.0
+    d.angpos[:] = 0.0
+    d.es[:] = 0.0
+    d.ev[:] = 0.0
+    d.xyzsum[:] = 0.0
+    low = d.x[:, 2] < (z_max - z_min) * 0.3
+    d_max_below = numpy.max(d.radius[low]) * 2.0
+    bottom = d.x[:, 2] < (z_min + d_max_below)
+    d.fixvel[bottom] = 1
+    high = d.x[:, 2] > (z_max - z_min) * 0.7
+    d_max_top = numpy.max(d.radius[high]) * 2.0
+    top = d.x[:, 2] > (z_max - d_max_top)
+    d.fixvel[top] = 1
+    d.vel[top, 0] = shear_velocity
+    add_top_wall(d, sigma0, wmode=1)
+    d.gamma_wt = 0.0
+    d.mu_ws = 0.0
+    d.mu_wd = 0.0
