@@ -1,0 +1,163 @@
+/*
+ * sphere_b200 -- C ABI of the B200 DEM step engine.
+ *
+ * The engine replaces what `sim.run()` reaches through a subprocess in the
+ * reference (python/sphere.py:4482-4540 -> src/main.cpp:28-211 ->
+ * DEM::DEM + DEM::startTime, src/sphere.cpp:16-95, src/device.cu:833-2834).
+ * Plain pointers and sizes only; every call returns a status code (0 = OK,
+ * < 0 = error, > 0 = warning) instead of exiting the process as the
+ * reference does (src/utility.cu:11-60).
+ *
+ * Ownership: the engine owns all device memory and its CUDA stream; callers
+ * own paths and host buffers.  A handle is used by one host thread at a time.
+ */
+#ifndef SPHERE_B200_H_
+#define SPHERE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sph_engine sph_engine;
+
+/* Status codes. */
+enum {
+    SPH_OK = 0,
+    SPH_WARN_NOCONV = 1,        /* Darcy solve hit maxiter (the reference continues) */
+    SPH_ERR_FILE = -1,          /* cannot open / short read / trailing bytes */
+    SPH_ERR_VERSION = -2,       /* format version is not 2.15 (src/file_io.cpp:47-54) */
+    SPH_ERR_INPUT = -3,         /* value check failed (src/sphere.cpp:145-345) */
+    SPH_ERR_CUDA = -4,          /* CUDA runtime error */
+    SPH_ERR_OUTSIDE = -5,       /* particle left the grid or became non-finite */
+    SPH_ERR_CAPACITY = -6,      /* contact slots exhausted (the reference drops silently) */
+    SPH_ERR_UNSUPPORTED = -7,   /* input uses a path this engine does not build */
+    SPH_ERR_ARG = -8,           /* bad argument / buffer size */
+    SPH_ERR_TIMEOUT = -9,       /* a bounded device wait gave up */
+};
+
+/* Arithmetic of the DEM step. */
+enum {
+    SPH_PREC_FAITHFUL = 0, /* FP64 with the reference's FP32 vector lengths */
+    SPH_PREC_FP64 = 1,     /* FP64 throughout (FP64 square roots) */
+    SPH_PREC_MIXED = 2,    /* FP32 contact kinematics and forces, FP64 overlap,
+                              accumulators, integration and reductions */
+};
+
+typedef struct sph_opts {
+    int fluid;            /* 1: the file has a fluid section (the reference's --fluid) */
+    int device;           /* CUDA device ordinal; -1 keeps the current device */
+    int verbose;          /* 1: progress on stdout like DEM::startTime */
+    int precision;        /* SPH_PREC_* */
+    int integrator;       /* 3: three-term Taylor (the reference's TY3), 2: two-term */
+    int contact_capacity; /* contact slots per particle; the reference's NC is 32 */
+    int warm_start;       /* Darcy: 0 previous-step guess, 1 learned warm start */
+    int graph_steps;      /* DEM steps captured per CUDA graph launch; 0 = automatic */
+    const char *output_dir; /* directory for .bin/status/conv outputs; NULL = "output" */
+} sph_opts;
+
+/* Fields for sph_get/sph_set.  Vector fields use the reference's Float4
+ * layout (4 doubles per particle, src/datatypes.h:16-33) in ORIGINAL
+ * particle order, so results compare directly with the reference's arrays. */
+typedef enum sph_field {
+    SPH_F_X = 0,        /* np x (x, y, z, radius) */
+    SPH_F_VEL,          /* np x (vx, vy, vz, fixvel) */
+    SPH_F_ANGVEL,       /* np x (wx, wy, wz, 0) */
+    SPH_F_ANGPOS,
+    SPH_F_FORCE,
+    SPH_F_TORQUE,
+    SPH_F_ACC,
+    SPH_F_ANGACC,
+    SPH_F_XYZSUM,
+    SPH_F_ES_DOT,       /* np doubles */
+    SPH_F_ES,
+    SPH_F_EV_DOT,
+    SPH_F_EV,
+    SPH_F_P,
+    SPH_F_CELLID,       /* np u32: sorted cell keys (thrust::sort_by_key output) */
+    SPH_F_INDEX,        /* np u32: original index of each sorted position */
+    SPH_F_CELLSTART,    /* ncells u32, 0xffffffff for empty cells */
+    SPH_F_CELLEND,      /* ncells u32 (valid where cellstart is not empty) */
+    SPH_F_CONTACTS,     /* np*capacity u32, keyed by original index; np = empty */
+    SPH_F_DELTA_T,      /* np*capacity x 4 doubles: tangential history */
+    SPH_F_DISTMOD,      /* np*capacity x 4 doubles: periodic shift + partner radius */
+    SPH_F_WALLS_NX,     /* nw x (nx, ny, nz, position) */
+    SPH_F_WALLS_MVFD,   /* nw x (mass, velocity, force, sigma0) */
+    SPH_F_WALLS_ACC,    /* nw doubles */
+    SPH_F_ITER,         /* 1 int64: DEM steps taken */
+    SPH_F_TIME,         /* 1 double: model time */
+    SPH_F_DARCY_P,      /* nx*ny*nz doubles, x fastest */
+    SPH_F_DARCY_PHI,
+    SPH_F_DARCY_DPHI,
+    SPH_F_DARCY_K,
+    SPH_F_DARCY_V,      /* nx*ny*nz x 3 doubles */
+    SPH_F_DARCY_F_P,    /* np x 4 doubles: pressure force on each particle */
+    SPH_F_DARCY_ITERS,  /* 1 int64: Jacobi iterations of the last fluid step */
+    SPH_F_DARCY_ITERS_TOTAL, /* 1 int64: Jacobi iterations since open */
+    SPH_F_BONDS,        /* nb0 x 2 u32 */
+    SPH_F_BONDS_DELTA,  /* nb0 x 4 doubles (t.x, t.y, t.z, n) */
+    SPH_F_BONDS_OMEGA,
+    SPH_F_COUNT
+} sph_field;
+
+typedef struct sph_info {
+    uint32_t np, nw, nb0, capacity;
+    uint32_t num[3];
+    int32_t periodic, contactmodel, precision, fluid;
+    int64_t iter;
+    double time, time_total, dt, file_dt;
+    uint32_t step_count;
+    int64_t resorts;      /* re-sorts performed (steps where a particle changed cell) */
+} sph_info;
+
+/* Fills *opts with the defaults (faithful FP64, TY3, 32 slots, device -1). */
+void sph_default_opts(sph_opts *opts);
+
+/* Reads and validates a .bin file (src/file_io.cpp:30-417 +
+ * src/sphere.cpp:145-345) and uploads the state.  Replaces `DEM dem(...)`
+ * at src/main.cpp:184. */
+int sph_open(const char *bin_path, const sph_opts *opts, sph_engine **out);
+
+/* Same as sph_open, from the bytes of a .bin file held in host memory. */
+int sph_open_buffer(const void *bytes, size_t nbytes, const sph_opts *opts,
+                    const char *sid, sph_engine **out);
+
+/* The full time loop with the reference's side effects: output files
+ * <out>/<sid>.output%05d.bin every file_dt, <sid>.status.dat, and
+ * <sid>-conv.log when fluid.  Replaces DEM::startTime (src/device.cu:833). */
+int sph_run(sph_engine *e);
+
+/* Advances n DEM steps without file output (benchmarks, parity tests). */
+int sph_step(sph_engine *e, uint64_t n);
+
+/* Number of bytes sph_get/sph_set move for a field (0 if not present). */
+int64_t sph_field_bytes(sph_engine *e, sph_field f);
+
+/* Copies a field to host memory (synchronises the engine's stream). */
+int sph_get(sph_engine *e, sph_field f, void *dst, size_t bytes);
+
+/* Overwrites a field from host memory (positions, velocities, ...). */
+int sph_set(sph_engine *e, sph_field f, const void *src, size_t bytes);
+
+/* Writes the current state as a .bin file (src/file_io.cpp:420-731). */
+int sph_write_bin(sph_engine *e, const char *path);
+
+int sph_get_info(sph_engine *e, sph_info *info);
+
+/* Message for the last non-zero status of this handle (never NULL). */
+const char *sph_last_error(sph_engine *e);
+
+/* Message for a failed sph_open (thread-local; never NULL). */
+const char *sph_open_error(void);
+
+void sph_close(sph_engine *e);
+
+/* Library build string: version, arch, compile flags of the DEM kernels. */
+const char *sph_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,71 @@
+"""Builds the engine library in-tree: sphere_b200/libsphere_b200.so.
+
+Every CUDA source is compiled for sm_100a only.  The FP64 DEM kernels are
+compiled with -fmad=false so their arithmetic rounds like the reference's
+--fmad=false build.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libsphere_b200.so")
+BUILD = os.path.join(HERE, "_build")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+# kernels whose results must round exactly like the reference
+NO_FMA = {"dem_kernels.cu", "sort.cu", "darcy.cu"}
+SOURCES = ["bin_io.cpp", "dem_kernels.cu", "sort.cu", "engine.cu", "darcy.cu", "dem_mixed.cu"]
+
+
+def nvcc() -> str:
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _needs(obj: str, deps) -> bool:
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose: bool = False, ptxas_info: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(HERE, "..", "include", "sphere_b200.h"))
+    objs = []
+    nv = nvcc()
+    for src in SOURCES:
+        path = os.path.join(CSRC, src)
+        obj = os.path.join(BUILD, src + ".o")
+        objs.append(obj)
+        if not _needs(obj, [path, __file__] + headers):
+            continue
+        cmd = [nv] + COMMON + ARCH + ["-c", path, "-o", obj]
+        if src.endswith(".cpp"):
+            cmd = [nv, "-x", "c++"] + COMMON + ["-c", path, "-o", obj]
+        if src in NO_FMA:
+            cmd.insert(1, "-fmad=false")
+        if ptxas_info and src.endswith(".cu"):
+            cmd += ["-Xptxas", "-v"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+    if _needs(OUT, objs):
+        cmd = [nv, "-shared"] + ARCH + ["-o", OUT] + objs + ["-lcuda"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(verbose=True, ptxas_info="-v" in sys.argv)

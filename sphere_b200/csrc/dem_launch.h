@@ -1,0 +1,31 @@
+// Host-side launchers of the DEM kernels.
+#pragma once
+
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "dem_state.h"
+
+namespace sphb {
+
+// prec: 0 faithful FP64 (FP32 lengths), 1 FP64.
+cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cudaStream_t st);
+cudaError_t launch_bonds(const DevParams &P, const DevState &S, int prec, double4 *bond_f,
+                         double4 *bond_t, cudaStream_t st);
+// shear-stress reduction (wmode 3), integration, wall reduction + wall
+// integration, loop counters
+cudaError_t launch_integrate(const DevParams &P, const DevState &S, cudaStream_t st);
+cudaError_t launch_hash(const DevParams &P, const DevState &S, cudaStream_t st);
+// force = 1 sorts unconditionally; otherwise only when DevCtl::resort is set
+cudaError_t launch_resort(const DevParams &P, const DevState &S, unsigned char *scratch,
+                          int force, cudaStream_t st);
+size_t resort_scratch_bytes(size_t np);
+
+// Gathers sorted storage into original order: dst[orig_of[k]] = src[k].
+cudaError_t launch_unsort(const void *src, void *dst, const uint32_t *orig_of, size_t np,
+                          size_t elem_bytes, cudaStream_t st);
+// Scatters original order into sorted storage: dst[k] = src[orig_of[k]].
+cudaError_t launch_sort_into(const void *src, void *dst, const uint32_t *orig_of, size_t np,
+                             size_t elem_bytes, cudaStream_t st);
+
+}  // namespace sphb

@@ -1,0 +1,92 @@
+// Engine object behind the C ABI.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "dem_state.h"
+#include "host_state.h"
+
+namespace sphb {
+
+struct DarcyDev;   // Darcy solver state (darcy.cu)
+struct MixedDev;   // mixed-precision state (dem_mixed.cu)
+
+class Engine {
+public:
+    ~Engine();
+
+    // options
+    int precision = 0;
+    int integrator = 3;
+    uint32_t capacity = 32;
+    int verbose = 0;
+    int graph_steps = 64;
+    int warm_start = 0;
+    std::string outdir = "output";
+    std::string sid = "unnamed";
+
+    HostState hs;
+    DevParams P{};
+    DevState S{};
+    cudaStream_t stream = nullptr;
+    std::vector<void *> allocations;
+    void *host_pinned = nullptr;
+    unsigned char *tmp = nullptr;
+    double4 *bond_f = nullptr, *bond_t = nullptr;
+
+    // loop state mirrored on the host (same double additions as the device)
+    double host_t = 0.0;
+    int64_t host_iter = 0;
+    DevCtl last_ctl{};
+
+    cudaGraphExec_t graph_exec = nullptr;
+    bool graph_failed = false;
+    bool warmed = false;
+
+    std::string err;
+
+    DarcyDev *darcy = nullptr;
+    MixedDev *mixed = nullptr;
+    FILE *convlog = nullptr;
+
+    int fail(int code, const std::string &msg);
+    int cuda_fail(cudaError_t e, const char *where);
+    template <class T> T *dalloc(size_t n);
+
+    void build_params();
+    int allocate_and_upload();
+    int poll_errors(const char *where);
+    cudaError_t enqueue_step();
+    int ensure_graph();
+    int step(uint64_t n);
+    void advance_host_clock(uint64_t n);
+    int64_t field_bytes(int f) const;
+    double4 *sorted_vec(int f) const;
+    double *sorted_scalar(int f) const;
+    int get(int f, void *dst, size_t bytes);
+    int get_distmod(double *dst);
+    int set(int f, const void *src, size_t bytes);
+    int download_state();
+    int write_bin(const char *path);
+    int write_status();
+    int run();
+
+    // Darcy (cfd_solver 1); no-ops for dry runs
+    int darcy_init();
+    int64_t darcy_field_bytes(int f) const;
+    int darcy_get(int f, void *dst, size_t bytes);
+    int darcy_download();
+    int step_with_fluid_log(uint64_t n);
+    void conv_open();
+    void conv_close();
+
+    // mixed precision
+    int mixed_init();
+};
+
+}  // namespace sphb

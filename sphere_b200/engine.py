@@ -1,0 +1,203 @@
+"""ctypes binding of the engine's C ABI (``include/sphere_b200.h``).
+
+The library is ``sphere_b200/libsphere_b200.so``, built in-tree by
+``sphere_b200/build.py``.  There is no fallback: if the library is missing
+or a CUDA device is unavailable, opening an engine raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Union
+
+import numpy
+
+from . import binfile
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsphere_b200.so")
+
+PREC = {"faithful": 0, "fp64": 1, "mixed": 2}
+
+FIELDS = [
+    "x", "vel", "angvel", "angpos", "force", "torque", "acc", "angacc", "xyzsum",
+    "es_dot", "es", "ev_dot", "ev", "p", "cellid", "index", "cellstart", "cellend",
+    "contacts", "delta_t", "distmod", "walls_nx", "walls_mvfd", "walls_acc", "iter",
+    "time", "darcy_p", "darcy_phi", "darcy_dphi", "darcy_k", "darcy_v", "darcy_f_p",
+    "darcy_iters", "darcy_iters_total", "bonds", "bonds_delta", "bonds_omega",
+]
+FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+_VEC4 = {"x", "vel", "angvel", "angpos", "force", "torque", "acc", "angacc", "xyzsum",
+         "delta_t", "distmod", "walls_nx", "walls_mvfd", "darcy_f_p", "bonds_delta",
+         "bonds_omega"}
+_U32 = {"cellid", "index", "cellstart", "cellend", "contacts", "bonds"}
+_I64 = {"iter", "darcy_iters", "darcy_iters_total"}
+
+STATUS = {
+    0: "ok", 1: "Darcy solve did not converge", -1: "file error", -2: "version",
+    -3: "input check failed", -4: "CUDA error", -5: "particle outside the grid",
+    -6: "contact capacity exceeded", -7: "unsupported input", -8: "bad argument",
+    -9: "device wait timed out",
+}
+
+
+class SphOpts(ctypes.Structure):
+    _fields_ = [("fluid", ctypes.c_int), ("device", ctypes.c_int), ("verbose", ctypes.c_int),
+                ("precision", ctypes.c_int), ("integrator", ctypes.c_int),
+                ("contact_capacity", ctypes.c_int), ("warm_start", ctypes.c_int),
+                ("graph_steps", ctypes.c_int), ("output_dir", ctypes.c_char_p)]
+
+
+class SphInfo(ctypes.Structure):
+    _fields_ = [("np", ctypes.c_uint32), ("nw", ctypes.c_uint32), ("nb0", ctypes.c_uint32),
+                ("capacity", ctypes.c_uint32), ("num", ctypes.c_uint32 * 3),
+                ("periodic", ctypes.c_int32), ("contactmodel", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("fluid", ctypes.c_int32),
+                ("iter", ctypes.c_int64), ("time", ctypes.c_double),
+                ("time_total", ctypes.c_double), ("dt", ctypes.c_double),
+                ("file_dt", ctypes.c_double), ("step_count", ctypes.c_uint32),
+                ("resorts", ctypes.c_int64)]
+
+
+class EngineError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS.get(status, status)} ({status}): {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads the engine library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m sphere_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    L.sph_default_opts.argtypes = [ctypes.POINTER(SphOpts)]
+    L.sph_open.argtypes = [ctypes.c_char_p, ctypes.POINTER(SphOpts), ctypes.POINTER(P)]
+    L.sph_open_buffer.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(SphOpts),
+                                  ctypes.c_char_p, ctypes.POINTER(P)]
+    L.sph_run.argtypes = [P]
+    L.sph_step.argtypes = [P, ctypes.c_uint64]
+    L.sph_field_bytes.argtypes = [P, ctypes.c_int]
+    L.sph_field_bytes.restype = ctypes.c_int64
+    L.sph_get.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
+    L.sph_set.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
+    L.sph_write_bin.argtypes = [P, ctypes.c_char_p]
+    L.sph_get_info.argtypes = [P, ctypes.POINTER(SphInfo)]
+    L.sph_last_error.argtypes = [P]
+    L.sph_last_error.restype = ctypes.c_char_p
+    L.sph_open_error.restype = ctypes.c_char_p
+    L.sph_close.argtypes = [P]
+    L.sph_version.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def make_opts(fluid=False, precision="faithful", integrator=3, capacity=32, device=-1,
+              graph_steps=0, warm_start=False, verbose=False, output_dir=None) -> SphOpts:
+    o = SphOpts()
+    lib().sph_default_opts(ctypes.byref(o))
+    o.fluid = int(bool(fluid))
+    o.precision = PREC[precision] if isinstance(precision, str) else int(precision)
+    o.integrator = int(integrator)
+    o.contact_capacity = int(capacity)
+    o.device = int(device)
+    o.graph_steps = int(graph_steps)
+    o.warm_start = int(bool(warm_start))
+    o.verbose = int(bool(verbose))
+    o.output_dir = os.fsencode(output_dir) if output_dir else None
+    return o
+
+
+class Engine:
+    """One simulation on the GPU.
+
+    ``source`` is a ``.bin`` path or a :class:`~sphere_b200.binfile.BinData`
+    (serialised in memory).  Vector fields come back in the reference's
+    Float4 layout, one row per particle in original order.
+    """
+
+    def __init__(self, source: Union[str, os.PathLike, binfile.BinData], fluid: Optional[bool] = None,
+                 precision="faithful", integrator=3, capacity=32, device=-1, graph_steps=0,
+                 warm_start=False, verbose=False, output_dir=None, sid=None):
+        L = lib()
+        h = ctypes.c_void_p()
+        if isinstance(source, binfile.BinData):
+            fl = source.fluid if fluid is None else fluid
+            self._opts = make_opts(fl, precision, integrator, capacity, device, graph_steps,
+                                   warm_start, verbose, output_dir)
+            buf = binfile.serialize_bin(source)
+            rc = L.sph_open_buffer(buf, len(buf), ctypes.byref(self._opts),
+                                   (sid or "unnamed").encode(), ctypes.byref(h))
+        else:
+            self._opts = make_opts(bool(fluid), precision, integrator, capacity, device,
+                                   graph_steps, warm_start, verbose, output_dir)
+            rc = L.sph_open(os.fsencode(source), ctypes.byref(self._opts), ctypes.byref(h))
+        if rc < 0 or not h.value:
+            raise EngineError(rc, L.sph_open_error().decode())
+        self._h = h
+        self.np = self.info().np
+
+    def _check(self, rc):
+        if rc < 0:
+            raise EngineError(rc, lib().sph_last_error(self._h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().sph_close(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def step(self, n=1) -> int:
+        return self._check(lib().sph_step(self._h, int(n)))
+
+    def run(self) -> int:
+        return self._check(lib().sph_run(self._h))
+
+    def info(self) -> SphInfo:
+        inf = SphInfo()
+        self._check(lib().sph_get_info(self._h, ctypes.byref(inf)))
+        return inf
+
+    def field_bytes(self, name) -> int:
+        return int(lib().sph_field_bytes(self._h, FIELD_ID[name]))
+
+    def get(self, name, out: Optional[numpy.ndarray] = None) -> numpy.ndarray:
+        nbytes = self.field_bytes(name)
+        if name in _VEC4:
+            dtype, shape = numpy.float64, (nbytes // 32, 4)
+        elif name in _U32:
+            dtype, shape = numpy.uint32, (nbytes // 4,)
+        elif name in _I64:
+            dtype, shape = numpy.int64, (nbytes // 8,)
+        elif name == "darcy_v":
+            dtype, shape = numpy.float64, (nbytes // 24, 3)
+        else:
+            dtype, shape = numpy.float64, (nbytes // 8,)
+        if out is None:
+            out = numpy.empty(shape, dtype=dtype)
+        self._check(lib().sph_get(self._h, FIELD_ID[name], out.ctypes.data, out.nbytes))
+        return out
+
+    def set(self, name, arr: numpy.ndarray) -> None:
+        arr = numpy.ascontiguousarray(arr)
+        self._check(lib().sph_set(self._h, FIELD_ID[name], arr.ctypes.data, arr.nbytes))
+
+    def write_bin(self, path) -> None:
+        self._check(lib().sph_write_bin(self._h, os.fsencode(path)))
