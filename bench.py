@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark of the DEM step: particle-steps/s on one B200.
+
+Workload: the dense-shear configuration -- N = 100,000 spheres, radii
+U(0.008, 0.012) m, settled packing, fixed bottom layer, top layer sheared at
+1e-4 m/s along x, top wall at sigma0 = 20 kPa, Young's modulus contact
+E = 7e8 Pa, mu = 0.5, periodic x/y (seeded synthetic data).
+
+One benchmark "step" is one output interval of INTERVAL DEM time steps (the
+unit `sim.run()` advances between two output files).  `value` is
+N * DEM steps / device time with the state resident on the GPU; `e2e` is the
+same metric through the C ABI with host buffers: every interval uploads the
+particle state (positions, velocities, angular velocities) from pinned host
+memory, advances INTERVAL DEM steps and reads the state back (positions,
+velocities, angular velocities, forces, torques).
+
+`python bench.py --impl reference` times the reference algorithm on the host
+cores instead: the CPU restatement of the reference's step (the oracle,
+OpenMP over all host threads; sphere has no CPU DEM path of its own) on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+INTERVAL = 100          # DEM steps per benchmark step
+N_PARTICLES = 100000
+SEED = 1
+
+
+def log(msg):
+    print(msg, file=sys.stderr, flush=True)
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.samples = []
+        self.proc = None
+        self.dev = device_index
+        self._thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self._thread = threading.Thread(target=self._read, daemon=True)
+        self._thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self._thread:
+            self._thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[1]))
+                mx = float(s[2])
+                for i, nm in enumerate(names):
+                    if s[5 + i].lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(numpy.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(n):
+    from sphere_b200 import configs
+    return configs.shear_benchmark(n=n, seed=SEED, log=log)
+
+
+def mean_contacts(eng, n):
+    c = eng.get("contacts")
+    return float((c != n).sum()) / n
+
+
+def flush_l2(buf):
+    buf.add_(1.0)
+
+
+def run_gpu(args):
+    import torch
+    from sphere_b200.engine import Engine
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n = args.particles
+    d = workload(n)
+    precision = args.precision
+    eng = Engine(d, precision=precision, graph_steps=INTERVAL)
+    # L2 flush buffer (256 MB, larger than the 126 MB L2)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        eng.step(INTERVAL)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing: value ----
+    sampler = ClockSampler()
+    sampler.start()
+    times = []
+    for _ in range(args.steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        # CUDA events on the engine's stream around the INTERVAL steps
+        times.append(eng.step_timed(INTERVAL) * 1e-3)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_s = float(numpy.sum(times))
+    value = n * INTERVAL * args.steps / step_s
+    zbar = mean_contacts(eng, n)
+
+    # ---- per-kernel timing with CUDA events (on the engine's stream) ----
+    prof = eng.profile(200)
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    x = torch.empty((n, 4), dtype=torch.float64).pin_memory()
+    vel = torch.empty((n, 4), dtype=torch.float64).pin_memory()
+    angvel = torch.empty((n, 4), dtype=torch.float64).pin_memory()
+    force = torch.empty((n, 4), dtype=torch.float64).pin_memory()
+    torque = torch.empty((n, 4), dtype=torch.float64).pin_memory()
+    xa, va, aa, fa, ta = (t.numpy() for t in (x, vel, angvel, force, torque))
+    eng.get("x", xa); eng.get("vel", va); eng.get("angvel", aa)
+    e2e_times = []
+    for _ in range(max(3, args.steps // 2)):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.set("x", xa); eng.set("vel", va); eng.set("angvel", aa)
+        eng.step(INTERVAL)
+        eng.get("x", xa); eng.get("vel", va); eng.get("angvel", aa)
+        eng.get("force", fa); eng.get("torque", ta)
+        t1 = time.perf_counter()
+        e2e_times.append(t1 - t0)
+    e2e_value = n * INTERVAL * len(e2e_times) / float(numpy.sum(e2e_times))
+    info = eng.info()
+    eng.close()
+
+    peak, peak_kind = load_peaks()
+    bytes_per_particle = 184.0 + 56.0 * zbar
+    contacts_bytes = n * bytes_per_particle
+    achieved = contacts_bytes / (prof.contacts_ms * 1e-3) / 1e9
+    launches_per_dem_step = 4 + (2 if d.nw > 0 and d.wmode[0] == 3 else 0)
+    out = {
+        "metric": "particle-steps/s",
+        "value": value,
+        "unit": "particle-steps/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * step_s / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if precision != "mixed" else "f32+f64",
+        "data": "synthetic (seeded settled packing)",
+        "config": {
+            "workload": f"dense dry shear, N={n}, radii U(0.008,0.012) m, E=7e8 Pa, "
+                        f"mu=0.5, sigma0=20 kPa, shear 1e-4 m/s, periodic x/y",
+            "dem_steps_per_step": INTERVAL,
+            "precision": precision,
+            "integrator": "TY3",
+            "mean_contacts_per_particle": zbar,
+            "l2": "flushed between timed steps (256 MB write)",
+        },
+        "e2e": {"value": e2e_value, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": 3 * 32 * n, "d2h_bytes_per_step": 5 * 32 * n},
+        "gpu_launches": launches_per_dem_step * INTERVAL * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "k_contacts (contact search + forces)",
+                     "bytes_per_particle": bytes_per_particle,
+                     "peak_source": peak_kind},
+        "stage_ms_per_dem_step": {"resort": prof.resort_ms, "contacts": prof.contacts_ms,
+                                  "bonds": prof.bonds_ms, "integrate": prof.integrate_ms,
+                                  "step": prof.step_ms},
+        "resorts": int(info.resorts),
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(d, sample_steps=args.cpu_steps)
+    return out
+
+
+def cpu_baseline(d, sample_steps=3):
+    """The oracle (CPU restatement of the reference step, OpenMP) on a
+    bounded sample of the same workload."""
+    import tempfile
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from sphere_b200 import binfile
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "w.bin")
+        binfile.write_bin(d, path)
+        orc = O.Oracle(path, precision="faithful")
+        orc.step(1)
+        t0 = time.perf_counter()
+        orc.step(sample_steps)
+        t1 = time.perf_counter()
+        orc.close()
+    cores = os.cpu_count() or 1
+    nthreads = int(os.environ.get("OMP_NUM_THREADS", cores))
+    return {"value": d.np * sample_steps / (t1 - t0), "unit": "particle-steps/s",
+            "cores": nthreads, "kind": "port",
+            "sample": f"{sample_steps} DEM steps of the N={d.np} workload after 1 warm-up step"}
+
+
+def run_reference(args):
+    n = args.particles
+    d = workload(n)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import tempfile
+    import oracle as O
+    from sphere_b200 import binfile
+    times = []
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "w.bin")
+        binfile.write_bin(d, path)
+        orc = O.Oracle(path, precision="faithful")
+        for _ in range(args.warmup):
+            orc.step(1)
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            rc = orc.step(args.ref_sample)
+            t1 = time.perf_counter()
+            if rc:
+                raise RuntimeError(orc.error())
+            times.append(t1 - t0)
+        orc.close()
+    total = float(numpy.sum(times))
+    value = n * args.ref_sample * args.steps / total
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = f"{args.ref_sample} DEM steps of the N={n} workload per benchmark step"
+    return {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded settled packing)",
+        "config": {"workload": f"dense dry shear, N={n}, radii U(0.008,0.012) m, E=7e8 Pa, "
+                               f"mu=0.5, sigma0=20 kPa, shear 1e-4 m/s, periodic x/y",
+                   "dem_steps_per_step": args.ref_sample},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--precision", default="faithful", choices=["faithful", "fp64", "mixed"])
+    ap.add_argument("--particles", type=int, default=N_PARTICLES)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--ref-sample", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args)), flush=True)
+        return 0
+    if world > 1:
+        # replicas only: every rank runs the same single-GPU workload; the
+        # timing is the max over ranks (see run_distributed)
+        return run_distributed(args, rank, world)
+    print(json.dumps(run_gpu(args)), flush=True)
+    return 0
+
+
+def run_distributed(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    args.no_cpu_baseline = rank != 0 or args.no_cpu_baseline
+    dist.barrier()
+    out = run_gpu(args)
+    t = torch.tensor([out["ms_per_step"]], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    if rank == 0:
+        ms = float(t.item())
+        out["ms_per_step"] = ms
+        out["value"] = world * args.particles * INTERVAL / (ms * 1e-3)
+        out["n_gpus"] = world
+        print(json.dumps(out), flush=True)
+    dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -132,6 +132,24 @@ int sph_run(sph_engine *e);
 /* Advances n DEM steps without file output (benchmarks, parity tests). */
 int sph_step(sph_engine *e, uint64_t n);
 
+/* Same as sph_step; *device_ms receives the device time of the n steps,
+ * measured with CUDA events recorded on the engine's stream. */
+int sph_step_timed(sph_engine *e, uint64_t n, double *device_ms);
+
+/* Per-kernel device time of the step, averaged over n DEM steps run
+ * eagerly with CUDA events around each stage (the reference's PROFILING
+ * table, src/device.cu:954-994,2717-2815).  The steps advance the run. */
+typedef struct sph_profile {
+    double resort_ms;     /* cell re-sort (skipped when no cell changed) */
+    double contacts_ms;   /* contact search + contact/wall forces */
+    double bonds_ms;      /* bond forces */
+    double fluid_ms;      /* Darcy solver */
+    double integrate_ms;  /* integration + wall reduction + wall update */
+    double step_ms;       /* whole step */
+    uint64_t steps;
+} sph_profile;
+int sph_profile_steps(sph_engine *e, uint64_t n, sph_profile *out);
+
 /* Number of bytes sph_get/sph_set move for a field (0 if not present). */
 int64_t sph_field_bytes(sph_engine *e, sph_field f);
 

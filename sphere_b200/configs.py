@@ -10,8 +10,8 @@ Workloads (the sizes of the published benchmark configurations):
 * :func:`settling_lattice` -- dry settling of N spheres on a cubic lattice
   (N = 10,000, radii U(0.009, 0.011) m, spacing 0.025 m, jitter +/-0.002 m,
   periodic x/y, linear contact k_n = k_t = 1.16e7 N/m, mu = 0.5).
-* :func:`shear_box` -- a dense packing under a top wall at normal stress
-  sigma0 with the top layer sheared along x (N = 100,000, radii
+* :func:`shear_benchmark` -- a settled packing under a top wall at normal
+  stress sigma0 with the top layer sheared along x (N = 100,000, radii
   U(0.008, 0.012) m, Young's modulus contact E = 7e8 Pa, mu = 0.5).
 * :func:`two_particle` / :func:`wall_particle` -- the reference's collision
   test set-ups (``tests/contactmodel.py``, ``tests/contactmodel_wall.py``).
@@ -165,33 +165,6 @@ def wall_particle(radius=1.0, z=1.05, vel0=-1.0, gamma_wn=0.0, E=0.0,
     return d
 
 
-def random_packing(n: int, seed: int, r_min: float, r_max: float,
-                   fill: float = 0.9, width_cells: int = 0) -> BinData:
-    """Jittered close-spaced lattice of n spheres (no overlaps), a cheap
-    stand-in for a settled packing: spacing 2*r_max*(1+gap), seeded radii."""
-    rng = numpy.random.default_rng(seed)
-    d = BinData()
-    _particles(d, n)
-    spacing = 2.0 * r_max * 1.002
-    side = int(math.ceil(math.sqrt(n / 1.0) ** (2.0 / 3.0))) if width_cells <= 0 else width_cells
-    side = max(side, 3)
-    nz = int(math.ceil(n / (side * side)))
-    idx = numpy.arange(n)
-    ix, iy, iz = idx % side, (idx // side) % side, idx // (side * side)
-    centres = numpy.column_stack([ix, iy, iz]).astype(numpy.float64)
-    jit = 0.001 * r_max
-    d.x = (centres + 0.5) * spacing + rng.uniform(-jit, jit, size=(n, 3))
-    d.radius = rng.uniform(r_min, r_max, size=n)
-    default_params(d, mu_s=0.5, mu_d=0.5, k_n=1.16e7, k_t=1.16e7)
-    d.g = numpy.array([0.0, 0.0, -9.81])
-    cell = 2.1 * r_max
-    Lxy = side * spacing
-    grid_for(d, L=[Lxy, Lxy, (nz + 2) * spacing], dx=Lxy / max(3, int(Lxy // cell)))
-    d.periodic = 1
-    _ = fill
-    return d
-
-
 def add_top_wall(d: BinData, sigma0: float, wmode: int = 1, mass=None) -> None:
     """One dynamic top wall at the highest particle surface
     (``sim.adjustUpperWall`` + ``consolidate``, ``python/sphere.py:2949-3048``)."""
@@ -239,3 +212,112 @@ def shear_setup(d: BinData, shear_velocity: float, sigma0: float) -> None:
     d.gamma_wt = 0.0
     d.mu_ws = 0.0
     d.mu_wd = 0.0
+
+
+def _lattice(n: int, seed: int, r_min: float, r_max: float, gap: float = 0.02):
+    """Jittered cubic lattice with spacing 2*r_max*(1+gap), roughly twice
+    as wide as tall; returns (x, radius, side, nz, spacing)."""
+    rng = numpy.random.default_rng(seed)
+    spacing = 2.0 * r_max * (1.0 + gap)
+    side = int(math.ceil((2.0 * n) ** (1.0 / 3.0)))
+    nz = int(math.ceil(n / (side * side)))
+    idx = numpy.arange(n)
+    ix, iy, iz = idx % side, (idx // side) % side, idx // (side * side)
+    centres = numpy.column_stack([ix, iy, iz]).astype(numpy.float64)
+    jit = 0.5 * gap * r_max
+    x = (centres + 0.5) * spacing + rng.uniform(-jit, jit, size=(n, 3))
+    radius = rng.uniform(r_min, r_max, size=n)
+    return x, radius, side, nz, spacing
+
+
+def settle_packing(n: int = 100000, seed: int = 1, r_min: float = 0.008,
+                   r_max: float = 0.012, g_factor: float = 100.0,
+                   max_steps: int = 60000, precision: str = "fp64",
+                   log=None) -> BinData:
+    """A settled packing made by damped DEM settling on the GPU engine.
+
+    Spheres start on a jittered lattice and settle under g_factor * 9.81
+    m/s^2 with strong normal and tangential damping and a 5x time step, then
+    relax at 1 g.  Used to make the dense starting state of the shear
+    workload (the 'prepacked by settling' step); it is not a timed path.
+    """
+    from .engine import Engine  # the GPU engine
+
+    x, radius, side, nz, spacing = _lattice(n, seed, r_min, r_max)
+    d = BinData()
+    _particles(d, n)
+    d.x = x
+    d.radius = radius
+    default_params(d, mu_s=0.5, mu_d=0.5, k_n=1.16e7, k_t=1.16e7)
+    m_min = d.rho * 4.0 / 3.0 * numpy.pi * r_min ** 3
+    d.gamma_n = 0.8 * 2.0 * math.sqrt(m_min * d.k_n)
+    d.gamma_t = 0.2 * d.gamma_n
+    d.gamma_wn = 4.0 * d.gamma_n
+    d.gamma_wt = 0.0
+    d.g = numpy.array([0.0, 0.0, -9.81 * g_factor])
+    L = side * spacing
+    grid_for(d, L=[L, L, (nz + 1) * spacing], dx=2.1 * r_max)
+    d.periodic = 1
+    d.time_dt = 5.0 * time_step(d)
+    d.time_total = 1e9
+    d.time_file_dt = 1e9
+    eng = Engine(d, precision=precision, graph_steps=100)
+    chunk = 2000
+    steps = 0
+    while steps < max_steps:
+        eng.step(chunk)
+        steps += chunk
+        v = eng.get("vel")[:, :3]
+        vmax = float(numpy.sqrt((v ** 2).sum(axis=1)).max())
+        if log:
+            log(f"settle: {steps} steps, max |v| {vmax:.3e} m/s")
+        if steps >= 20000 and vmax < 0.05:
+            break
+    state = d.copy()
+    xs = eng.get("x")
+    state.x = xs[:, :3].copy()
+    eng.close()
+    state.vel[:] = 0.0
+    state.angvel[:] = 0.0
+    state.g = numpy.array([0.0, 0.0, -9.81])
+    top = float(numpy.max(state.x[:, 2] + state.radius))
+    state.L = state.L.copy()
+    state.num = state.num.copy()
+    cell = state.L[0] / state.num[0]
+    state.num[2] = int(math.ceil(top * 1.1 / cell))
+    state.L[2] = state.num[2] * cell
+    return state
+
+
+def shear_benchmark(n: int = 100000, seed: int = 1, sigma0: float = 20e3,
+                    shear_velocity: float = 1e-4, cache_dir=None, log=None) -> BinData:
+    """The dense-shear workload: a settled packing of n spheres (radii
+    U(0.008, 0.012) m), fixed bottom layer, top layer sheared at
+    shear_velocity along x, one top wall at normal stress sigma0, Young's
+    modulus contact E = 7e8 Pa, mu = 0.5, periodic x/y.  The settled packing
+    is cached as a .bin file under cache_dir."""
+    import os
+    from .binfile import read_bin, write_bin
+
+    cache_dir = cache_dir or os.environ.get("SPHB_CACHE", "/tmp/sphere_b200_cache")
+    os.makedirs(cache_dir, exist_ok=True)
+    path = os.path.join(cache_dir, f"packing_n{n}_seed{seed}.bin")
+    if os.path.exists(path):
+        base = read_bin(path)
+    else:
+        base = settle_packing(n=n, seed=seed, log=log)
+        write_bin(base, path + ".tmp")
+        os.replace(path + ".tmp", path)
+    d = base.copy()
+    default_params(d, mu_s=0.5, mu_d=0.5, k_n=1.16e7, k_t=1.16e7)
+    d.E = 7e8
+    d.gamma_n = 0.0
+    d.gamma_t = 0.0
+    d.gamma_wn = 1.0e4
+    d.gamma_wt = 1.0e4
+    shear_setup(d, shear_velocity, sigma0)
+    d.time_dt = time_step(d)
+    d.time_current = 0.0
+    d.time_total = 50000 * d.time_dt
+    d.time_file_dt = d.time_total
+    return d

@@ -268,14 +268,66 @@ int Engine::poll_errors(const char *where)
     }
 }
 
+cudaError_t Engine::enqueue_stage(int stage)
+{
+    const int prec = precision == 0 ? 0 : 1;
+    switch (stage) {
+    case 0: return launch_resort(P, S, S.perm_scratch, 0, stream);
+    case 1: return launch_contacts(P, S, prec, stream);
+    case 2: return launch_bonds(P, S, prec, bond_f, bond_t, stream);
+    case 3: return enqueue_fluid();
+    case 4: return launch_integrate(P, S, stream);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t Engine::enqueue_step()
 {
-    cudaError_t e;
-    if ((e = launch_resort(P, S, S.perm_scratch, 0, stream)) != cudaSuccess) return e;
-    if ((e = launch_contacts(P, S, precision == 0 ? 0 : 1, stream)) != cudaSuccess) return e;
-    if ((e = launch_bonds(P, S, precision == 0 ? 0 : 1, bond_f, bond_t, stream)) != cudaSuccess) return e;
-    if ((e = launch_integrate(P, S, stream)) != cudaSuccess) return e;
+    for (int st = 0; st < 5; ++st) {
+        cudaError_t e = enqueue_stage(st);
+        if (e != cudaSuccess) return e;
+    }
     return cudaSuccess;
+}
+
+int Engine::profile(uint64_t n, sph_profile *out)
+{
+    std::memset(out, 0, sizeof *out);
+    cudaEvent_t ev[6];
+    for (auto &x : ev) cudaEventCreate(&x);
+    double ms[5] = {0, 0, 0, 0, 0}, total = 0;
+    int rc = ST_OK;
+    for (uint64_t i = 0; i < n && rc == ST_OK; ++i) {
+        cudaEventRecord(ev[0], stream);
+        for (int st = 0; st < 5; ++st) {
+            cudaError_t e = enqueue_stage(st);
+            if (e != cudaSuccess) { rc = cuda_fail(e, "profile"); break; }
+            cudaEventRecord(ev[st + 1], stream);
+        }
+        if (rc) break;
+        cudaEventSynchronize(ev[5]);
+        for (int st = 0; st < 5; ++st) {
+            float t = 0;
+            cudaEventElapsedTime(&t, ev[st], ev[st + 1]);
+            ms[st] += t;
+        }
+        float t = 0;
+        cudaEventElapsedTime(&t, ev[0], ev[5]);
+        total += t;
+        advance_host_clock(1);
+        warmed = true;
+    }
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (rc) return rc;
+    double inv = n ? 1.0 / (double)n : 0.0;
+    out->resort_ms = ms[0] * inv;
+    out->contacts_ms = ms[1] * inv;
+    out->bonds_ms = ms[2] * inv;
+    out->fluid_ms = ms[3] * inv;
+    out->integrate_ms = ms[4] * inv;
+    out->step_ms = total * inv;
+    out->steps = n;
+    return poll_errors("profile");
 }
 
 int Engine::ensure_graph()
@@ -709,7 +761,36 @@ const char *sph_open_error(void) { return sphb::g_open_error.c_str(); }
 
 int sph_run(sph_engine *e) { return e ? e->e->run() : SPH_ERR_ARG; }
 
+int sph_profile_steps(sph_engine *e, uint64_t n, sph_profile *out)
+{
+    return (e && out) ? e->e->profile(n, out) : SPH_ERR_ARG;
+}
+
 int sph_step(sph_engine *e, uint64_t n) { return e ? e->e->step_with_fluid_log(n) : SPH_ERR_ARG; }
+
+int sph_step_timed(sph_engine *e, uint64_t n, double *device_ms)
+{
+    if (!e || !device_ms) return SPH_ERR_ARG;
+    Engine &g = *e->e;
+    if (!g.warmed && n > 0) {
+        int rc = g.step_with_fluid_log(1);
+        if (rc < 0) return rc;
+        --n;
+    }
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, g.stream);
+    int rc = g.step_with_fluid_log(n);
+    cudaEventRecord(b, g.stream);
+    cudaEventSynchronize(b);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *device_ms = ms;
+    return rc;
+}
 
 int64_t sph_field_bytes(sph_engine *e, sph_field f)
 {

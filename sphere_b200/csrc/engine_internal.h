@@ -10,6 +10,7 @@
 
 #include "dem_state.h"
 #include "host_state.h"
+#include "../../include/sphere_b200.h"
 
 namespace sphb {
 
@@ -61,7 +62,10 @@ public:
     void build_params();
     int allocate_and_upload();
     int poll_errors(const char *where);
+    cudaError_t enqueue_stage(int stage);
     cudaError_t enqueue_step();
+    cudaError_t enqueue_fluid();
+    int profile(uint64_t n, struct sph_profile *out);
     int ensure_graph();
     int step(uint64_t n);
     void advance_host_clock(uint64_t n);

@@ -58,6 +58,13 @@ class SphInfo(ctypes.Structure):
                 ("resorts", ctypes.c_int64)]
 
 
+class SphProfile(ctypes.Structure):
+    _fields_ = [("resort_ms", ctypes.c_double), ("contacts_ms", ctypes.c_double),
+                ("bonds_ms", ctypes.c_double), ("fluid_ms", ctypes.c_double),
+                ("integrate_ms", ctypes.c_double), ("step_ms", ctypes.c_double),
+                ("steps", ctypes.c_uint64)]
+
+
 class EngineError(RuntimeError):
     def __init__(self, status, message):
         super().__init__(f"{STATUS.get(status, status)} ({status}): {message}")
@@ -82,6 +89,8 @@ def lib() -> ctypes.CDLL:
                                   ctypes.c_char_p, ctypes.POINTER(P)]
     L.sph_run.argtypes = [P]
     L.sph_step.argtypes = [P, ctypes.c_uint64]
+    L.sph_step_timed.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
+    L.sph_profile_steps.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(SphProfile)]
     L.sph_field_bytes.argtypes = [P, ctypes.c_int]
     L.sph_field_bytes.restype = ctypes.c_int64
     L.sph_get.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
@@ -166,6 +175,19 @@ class Engine:
 
     def step(self, n=1) -> int:
         return self._check(lib().sph_step(self._h, int(n)))
+
+    def step_timed(self, n) -> float:
+        """Advances n steps; returns their device time in ms (CUDA events on
+        the engine's stream)."""
+        ms = ctypes.c_double(0.0)
+        self._check(lib().sph_step_timed(self._h, int(n), ctypes.byref(ms)))
+        return ms.value
+
+    def profile(self, n) -> SphProfile:
+        """Per-stage device time per DEM step over n eager steps."""
+        p = SphProfile()
+        self._check(lib().sph_profile_steps(self._h, int(n), ctypes.byref(p)))
+        return p
 
     def run(self) -> int:
         return self._check(lib().sph_run(self._h))

@@ -1,0 +1,137 @@
+"""The .bin v2.15 codec: round trips, the reference's shipped fixtures,
+upgrades from 2.11, truncation/version errors, and byte equality with the
+reference's own Python writer (python/sphere.py:1355-1553) where the
+reference tree is present."""
+import os
+import sys
+import types
+
+import numpy
+import pytest
+
+from sphere_b200 import binfile, configs
+
+REF_PY = "/root/reference/python"
+REF_OUT = "/root/reference/output"
+
+
+def test_roundtrip_dry():
+    d = configs.settling_lattice(n=200, seed=3, nx=6, ny=6, nz=6)
+    buf = binfile.serialize_bin(d)
+    e = binfile.parse_bin(buf)
+    assert binfile.serialize_bin(e) == buf
+    assert e.np == 200 and numpy.array_equal(e.x, d.x)
+
+
+def test_roundtrip_walls_bonds():
+    d = configs.settling_lattice(n=150, seed=4, nx=6, ny=6, nz=6)
+    configs.shear_setup(d, 1e-3, 20e3)
+    d.nb0 = 3
+    d.bonds = numpy.array([[0, 1], [2, 3], [4, 5]], dtype=numpy.uint32)
+    d.bonds_delta_n = numpy.arange(3.0)
+    d.bonds_delta_t = numpy.ones((3, 3))
+    d.bonds_omega_n = -numpy.arange(3.0)
+    d.bonds_omega_t = numpy.full((3, 3), 2.0)
+    buf = binfile.serialize_bin(d)
+    e = binfile.parse_bin(buf)
+    assert binfile.serialize_bin(e) == buf
+    assert e.nw == 1 and e.wmode[0] == 1 and e.nb0 == 3
+
+
+def test_roundtrip_fluid():
+    d = configs.settling_lattice(n=100, seed=5, nx=5, ny=5, nz=5)
+    nx, ny, nz = (int(v) for v in d.num)
+    d.fluid = True
+    d.cfd_solver = 1
+    d.mu = 1.797e-6
+    rng = numpy.random.default_rng(0)
+    d.v_f = rng.normal(size=(nx, ny, nz, 3))
+    d.p_f = rng.normal(size=(nx, ny, nz))
+    d.phi = rng.uniform(0.3, 0.6, size=(nx, ny, nz))
+    d.dphi = numpy.zeros((nx, ny, nz))
+    d.p_f_constant = numpy.zeros((nx, ny, nz), dtype=numpy.int32)
+    d.p_f_constant[0, 1, 2] = 1
+    d.f_p = numpy.zeros((d.np, 3))
+    buf = binfile.serialize_bin(d)
+    e = binfile.parse_bin(buf, fluid=True)
+    assert binfile.serialize_bin(e) == buf
+    assert numpy.array_equal(e.p_f, d.p_f) and e.p_f_constant[0, 1, 2] == 1
+    # fluid auto-detection from the trailing byte count
+    assert binfile.parse_bin(buf).fluid
+
+
+def test_errors():
+    d = configs.settling_lattice(n=50, seed=6, nx=4, ny=4, nz=4)
+    buf = binfile.serialize_bin(d)
+    with pytest.raises(binfile.BinFormatError):
+        binfile.parse_bin(buf[:-10])
+    with pytest.raises(binfile.BinFormatError):
+        binfile.parse_bin(numpy.float64(2.14).tobytes() + buf[8:])
+    with pytest.raises(binfile.BinFormatError):
+        binfile.parse_bin(buf + b"\0\0\0\0", fluid=False)
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_OUT), reason="reference fixtures not present")
+@pytest.mark.parametrize("name,np_expected", [("init-1e4.output00199.bin", 10000),
+                                               ("cube-init.output00029.bin", 1000)])
+def test_reference_fixtures_upgrade(tmp_path, name, np_expected):
+    src = os.path.join(REF_OUT, name)
+    dst = str(tmp_path / "up.bin")
+    d = binfile.upgrade_to_215(src, dst)
+    assert d.np == np_expected
+    e = binfile.read_bin(dst)
+    assert e.version == 2.15 and e.adaptive == 0 and e.E == 0.0
+    assert numpy.array_equal(e.x, d.x) and numpy.array_equal(e.radius, d.radius)
+    with pytest.raises(binfile.BinFormatError):
+        binfile.read_bin(src)  # 2.11 is rejected like the reference does
+
+
+def _import_reference_sphere():
+    """Imports python/sphere.py read-only with stand-ins for what it needs
+    but does not use here: matplotlib, and numpy.infty (NumPy 2)."""
+    if not os.path.isdir(REF_PY):
+        pytest.skip("reference python tree not present")
+    for m in ("matplotlib", "matplotlib.pyplot", "matplotlib.collections",
+              "matplotlib.colors", "matplotlib.cm", "matplotlib.patches",
+              "matplotlib.ticker", "matplotlib.font_manager"):
+        sys.modules.setdefault(m, types.ModuleType(m))
+    mpl = sys.modules["matplotlib"]
+    mpl.use = lambda *a, **k: None
+    mpl.rc = lambda *a, **k: None
+    mpl.rcParams = {}
+    sys.modules["matplotlib.font_manager"].FontProperties = object
+    if not hasattr(numpy, "infty"):
+        numpy.infty = numpy.inf
+    sys.path.insert(0, REF_PY)
+    try:
+        import sphere
+    finally:
+        sys.path.remove(REF_PY)
+    return sphere
+
+
+class _Count(numpy.ndarray):
+    """1-element count arrays that work in range() (sphere.py predates NumPy 2)."""
+
+    def __index__(self):
+        return int(self[0])
+
+
+def test_writer_matches_reference_python_writer(tmp_path):
+    sphere = _import_reference_sphere()
+    n = 40
+    sim = sphere.sim(np=n, sid="codec")
+    sim.np = numpy.asarray(sim.np).view(_Count)
+    rng = numpy.random.default_rng(9)
+    sim.radius[:] = rng.uniform(0.01, 0.02, n)
+    sim.x[:, :] = rng.uniform(0.1, 0.9, (n, 3))
+    sim.vel[:, :] = rng.normal(size=(n, 3))
+    sim.defineWorldBoundaries(L=[1.0, 1.0, 1.0])
+    sim.setYoungsModulus(7e8)
+    sim.initTemporal(total=0.01, file_dt=0.001)
+    sim.writebin(folder=str(tmp_path), verbose=False)
+    ref_bytes = open(tmp_path / "codec.bin", "rb").read()
+    d = binfile.parse_bin(ref_bytes)
+    assert binfile.serialize_bin(d) == ref_bytes
+    assert d.E == 7e8 and d.np == n
+    assert d.time_dt == pytest.approx(configs.time_step(d), rel=0, abs=0)

@@ -1,0 +1,46 @@
+"""The oracle reproduces the reference's own outputs (tests/golden, made by
+running the reference kernels through oracle/_ref) bit for bit."""
+import glob
+import os
+
+import numpy
+import pytest
+
+import oracle as O
+from helpers import VEC3, bits_equal, diff_report
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(HERE, "*.bin")))
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built():
+    O.build(ref=False)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_matches_reference_golden(case):
+    gold = numpy.load(os.path.join(HERE, case + ".npz"))
+    steps = sorted({int(k.split("@")[1]) for k in gold.files})
+    fields = sorted({k.split("@")[0] for k in gold.files})
+    orc = O.Oracle(os.path.join(HERE, case + ".bin"))
+    done = 0
+    for s in steps:
+        assert orc.step(s - done) == 0, orc.error()
+        done = s
+        for f in fields:
+            a = orc.get(f)
+            if f in VEC3:
+                a = a[:, :3]
+            b = gold[f"{f}@{s}"]
+            assert bits_equal(a, b), f"step {s}: " + diff_report(f, a, b)
+    orc.close()
+
+
+def test_golden_cases_have_contacts():
+    for case in CASES:
+        gold = numpy.load(os.path.join(HERE, case + ".npz"))
+        if case == "dense_model1":
+            continue
+        n = gold["x@1"].shape[0]
+        assert (gold["contacts@20"] != n).sum() > 50, case
