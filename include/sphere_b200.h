@@ -172,6 +172,33 @@ const char *sph_open_error(void);
 
 void sph_close(sph_engine *e);
 
+/* Cell sort without allocation.  This entry point has no counterpart in the
+ * reference; it exists for callers that cannot allocate device memory --
+ * for example a host application whose own memory pool owns the GPU and
+ * forbids outside cudaMalloc, or a time-critical loop that must not call
+ * cudaMalloc/cudaFree because those calls synchronise the device.  It
+ * computes what the engine's sort computes: for np positions x4 (device
+ * pointer, np x (x, y, z, radius) doubles, original order) on the grid
+ * (origo, L, num), the stable cell sort -- cellid[np] sorted cell keys,
+ * index[np] original indices, cell_start/cell_end[num0*num1*num2]
+ * (0xffffffff start for empty cells) -- all device pointers the caller owns.
+ * Its scratch is one static device array built into the library
+ * (SPH_NOALLOC_MAX_CELLS cells, about 8.4 MB on every GPU that loads the
+ * library, held until exit); larger grids are rejected with SPH_ERR_ARG.
+ * The first call on a device looks the array up on that device
+ * (cudaGetSymbolAddress); later calls reuse it.  Every call shares that one
+ * array, so calls whose work overlaps on the GPU (another stream, another
+ * thread) race: serialise them.  `stream` is a cudaStream_t (NULL = legacy
+ * default stream); the call waits for its own work.  Returns SPH_OK,
+ * SPH_ERR_ARG, SPH_ERR_OUTSIDE (a position outside the grid) or
+ * SPH_ERR_CUDA; sph_noalloc_error() describes the last failure. */
+#define SPH_NOALLOC_MAX_CELLS (1u << 20)
+int sph_sort_cells_noalloc(const double *x4, uint32_t np, const double origo[3],
+                           const double L[3], const uint32_t num[3], uint32_t *cellid,
+                           uint32_t *index, uint32_t *cell_start, uint32_t *cell_end,
+                           void *stream);
+const char *sph_noalloc_error(void);
+
 /* Library build string: version, arch, compile flags of the DEM kernels. */
 const char *sph_version(void);
 

@@ -20,7 +20,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 # kernels whose results must round exactly like the reference
 NO_FMA = {"dem_kernels.cu", "sort.cu", "darcy.cu"}
-SOURCES = ["bin_io.cpp", "dem_kernels.cu", "sort.cu", "engine.cu", "darcy.cu", "dem_mixed.cu"]
+SOURCES = ["bin_io.cpp", "dem_kernels.cu", "sort.cu", "engine.cu", "darcy.cu", "dem_mixed.cu",
+           "noalloc_sort.cu"]
 
 
 def nvcc() -> str:
