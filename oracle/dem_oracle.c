@@ -51,9 +51,12 @@ double orc_sqrtf(const orc_state *s, double v)
 
 void orc_set_error(orc_state *s, int code, const char *msg)
 {
-    if (s->err == 0) {
-        s->err = code;
-        snprintf(s->errmsg, sizeof(s->errmsg), "%s", msg);
+#pragma omp critical(orc_error)
+    {
+        if (s->err == 0) {
+            s->err = code;
+            snprintf(s->errmsg, sizeof(s->errmsg), "%s", msg);
+        }
     }
 }
 
@@ -220,12 +223,17 @@ static void topology_particle(orc_state *s, unsigned a)
                         s->distmod[(size_t)a_orig * NCs + cpos] = dmv;
                         ++nc;
                         if (nc > (int)NCs) {
+                            /* More overlapping partners than slots: the
+                             * reference stops scanning this cell and drops
+                             * contacts silently (contactsearch.cuh:298-299);
+                             * the oracle reports it. */
                             s->capacity_hit = 1;
-                            goto next_cell; /* early return from this cell */
+                            orc_set_error(s, ORC_ERR_CAPACITY,
+                                          "more overlapping partners than contact slots");
+                            return;
                         }
                     }
                 }
-            next_cell:;
             }
 }
 

@@ -232,7 +232,7 @@ def _lattice(n: int, seed: int, r_min: float, r_max: float, gap: float = 0.02):
 
 def settle_packing(n: int = 100000, seed: int = 1, r_min: float = 0.008,
                    r_max: float = 0.012, g_factor: float = 100.0,
-                   max_steps: int = 60000, precision: str = "fp64",
+                   max_steps: int = 40000, precision: str = "fp64",
                    log=None) -> BinData:
     """A settled packing made by damped DEM settling on the GPU engine.
 

@@ -186,20 +186,107 @@ __device__ __forceinline__ void grid_pos(const DevParams &P, double4 x, int &gx,
 
 // ---------------------------------------------------------------------
 // contact search + forces: topology (contactsearch.cuh:329-371) and
-// interact (contactsearch.cuh:385-726) for one particle per thread.  The
-// slot row of the particle stays in shared memory between the two phases;
-// this is the reference's topology-then-interact order because each
-// particle's row is private to its thread.
+// interact (contactsearch.cuh:385-726) for one particle per thread.
+//
+// Candidates come from a neighbour list built in the reference's visiting
+// order (27 cells z, y, x; sorted order inside a cell) holding every pair
+// closer than r_a + r_b + skin.  The list is rebuilt whenever the sort
+// changed or a particle moved more than 0.45 skin since the build, so a
+// pair missing from it cannot overlap: the overlap tests, and therefore the
+// slot insertions, happen in exactly the reference's sequence.  The slot
+// row is tracked with an occupancy bitmask so the slot policy and the force
+// loop visit occupied slots only; empty slots keep zero history, which is
+// what the reference rewrites into them every step.
 // ---------------------------------------------------------------------
+constexpr uint32_t NL_OVERFLOW = 0xffffffffu;
+
+__device__ __forceinline__ V3 shift_vec(const DevParams &P, int sx, int sy)
+{
+    V3 dm = mk3(0.0, 0.0, 0.0);
+    if (sx > 0) dm = add3(dm, mk3(P.L[0], 0.0, 0.0));
+    if (sx < 0) dm = sub3(dm, mk3(P.L[0], 0.0, 0.0));
+    if (sy > 0) dm = add3(dm, mk3(0.0, P.L[1], 0.0));
+    if (sy < 0) dm = sub3(dm, mk3(0.0, P.L[1], 0.0));
+    return dm;
+}
+
+// Visits every candidate of particle k in the reference's 27-cell order and
+// calls f(b, sx, sy) with its sorted index and periodic shift signs.
+template <class F>
+__device__ __forceinline__ void for_each_cell_candidate(const DevParams &P, const DevState &S,
+                                                        unsigned k, double4 xa, F &&f)
+{
+    int gx, gy, gz;
+    grid_pos(P, xa, gx, gy, gz);
+    for (int dz = -1; dz < 2; ++dz)
+        for (int dy = -1; dy < 2; ++dy)
+            for (int dx = -1; dx < 2; ++dx) {
+                int cx = gx + dx, cy = gy + dy, cz = gz + dz, sx, sy;
+                if (!wrap_cell(P, cx, cy, cz, sx, sy)) continue;
+                unsigned cell = (unsigned)cx + (unsigned)cy * P.num[0] +
+                                (P.num[0] * P.num[1]) * (unsigned)cz;
+                unsigned start = S.cell_start[cell];
+                if (start == 0xffffffffu) continue;
+                unsigned end = S.cell_end[cell];
+                for (unsigned b = start; b < end; ++b) {
+                    if (b == k) continue;
+                    if (!f(b, sx, sy)) return;
+                }
+            }
+}
+
+// Neighbour list build: runs every step, works only when DevCtl::nl_rebuild.
+__global__ void __launch_bounds__(128) k_nl_build(DevParams P, DevState S)
+{
+    unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (S.ctl->err || !S.ctl->nl_rebuild || k >= P.np) return;
+    double4 xa = S.x[k];
+    const double ra = xa.w;
+    unsigned n = 0;
+    const size_t np = P.np;
+    for_each_cell_candidate(P, S, k, xa, [&](unsigned b, int sx, int sy) {
+        double4 xb = S.x[b];
+        V3 dm = shift_vec(P, sx, sy);
+        V3 xab = add3(mk3(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z), dm);
+        double reach = ra + xb.w + P.skin;
+        if (dot3(xab, xab) < reach * reach) {
+            if (n < P.nlmax) S.nl[(size_t)n * np + k] = b | ((uint32_t)dm_encode(sx, sy) << 28);
+            ++n;
+        }
+        return true;
+    });
+    S.nl_count[k] = n <= P.nlmax ? n : NL_OVERFLOW;
+    S.x_ref[k] = make_float4((float)xa.x, (float)xa.y, (float)xa.z, 0.0f);
+    if (k == 0) S.ctl->nl_builds += 1;
+}
+
+// The slot the reference's topology picks for partner b_orig
+// (contactsearch.cuh:267-280): the first slot already holding b_orig, else
+// the last empty slot, else nc.
+__device__ __forceinline__ int pick_slot(uint64_t mask, uint64_t full, const uint32_t *srow,
+                                         unsigned B, unsigned t, unsigned b_orig, int nc)
+{
+    uint64_t m = mask;
+    while (m) {
+        int i = __ffsll((long long)m) - 1;
+        if (srow[i * B + t] == b_orig) return i;
+        m &= m - 1;
+    }
+    uint64_t empty = ~mask & full;
+    if (empty) return 63 - __clzll((long long)empty);
+    return nc;
+}
+
 template <int PREC, int MODEL>
 __global__ void __launch_bounds__(128) k_contacts(DevParams P, DevState S)
 {
     extern __shared__ uint32_t srow[];
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (S.ctl->err) return;
-    if (k >= P.np) return;
+    if (k == 0 && S.ctl->nl_rebuild) S.ctl->nl_rebuild = 0;  // k_nl_build has run
+    if (S.ctl->err || k >= P.np) return;
     const unsigned B = blockDim.x, t = threadIdx.x;
     const unsigned NC = P.nc;
+    const uint64_t full = NC >= 64 ? ~0ull : ((1ull << NC) - 1ull);
     const unsigned o = S.orig_of[k];
     const double4 xa = S.x[k];
     const double ra = xa.w;
@@ -207,64 +294,67 @@ __global__ void __launch_bounds__(128) k_contacts(DevParams P, DevState S)
     const V3 angvel_a = xyz(S.angvel[k]);
     double es_dot = 0.0, ev_dot = 0.0, p = 0.0;
     V3 F = mk3(0.0, 0.0, 0.0), T = mk3(0.0, 0.0, 0.0);
+    const unsigned cnt = S.nl_count[k];
+    const size_t np = P.np;
 
     if (MODEL == 2) {
         const size_t rowbase = (size_t)o * NC;
-        for (unsigned i = 0; i < NC; ++i) srow[i * B + t] = S.contacts[rowbase + i];
-        bool dirty = false;
+        uint64_t mask = S.occ[o];
+        uint64_t written = 0;
+        {
+            uint64_t m = mask;
+            while (m) {
+                int i = __ffsll((long long)m) - 1;
+                srow[i * B + t] = S.contacts[rowbase + i];
+                m &= m - 1;
+            }
+        }
         // --- topology ---
         int nc = 0;
-        int gx, gy, gz;
-        grid_pos(P, xa, gx, gy, gz);
-        for (int dz = -1; dz < 2; ++dz)
-            for (int dy = -1; dy < 2; ++dy)
-                for (int dx = -1; dx < 2; ++dx) {
-                    int cx = gx + dx, cy = gy + dy, cz = gz + dz, sx, sy;
-                    if (!wrap_cell(P, cx, cy, cz, sx, sy)) continue;
-                    V3 dm = mk3(0.0, 0.0, 0.0);
-                    if (sx > 0) dm = add3(dm, mk3(P.L[0], 0.0, 0.0));
-                    if (sx < 0) dm = sub3(dm, mk3(P.L[0], 0.0, 0.0));
-                    if (sy > 0) dm = add3(dm, mk3(0.0, P.L[1], 0.0));
-                    if (sy < 0) dm = sub3(dm, mk3(0.0, P.L[1], 0.0));
-                    unsigned cell = (unsigned)cx + (unsigned)cy * P.num[0] +
-                                    (P.num[0] * P.num[1]) * (unsigned)cz;
-                    unsigned start = S.cell_start[cell];
-                    if (start == 0xffffffffu) continue;
-                    unsigned end = S.cell_end[cell];
-                    for (unsigned b = start; b < end; ++b) {
-                        if (b == k) continue;
-                        double4 xb = S.x[b];
-                        double rb = xb.w;
-                        V3 xab = mk3(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
-                        xab = add3(xab, dm);
-                        double len = vlen<PREC>(xab);
-                        double delta = len - (ra + rb);
-                        if (delta < 0.0) {
-                            unsigned b_orig = S.orig_of[b];
-                            int cpos = nc;
-                            for (unsigned i = 0; i < NC; ++i) {
-                                unsigned c = srow[i * B + t];
-                                if (c == P.np) cpos = (int)i;
-                                else if (c == b_orig) { cpos = (int)i; break; }
-                            }
-                            if (cpos >= (int)NC) {
-                                raise_err(S.ctl, DERR_CAPACITY, (int)o);
-                                return;
-                            }
-                            srow[cpos * B + t] = b_orig;
-                            S.dmcode[rowbase + cpos] = dm_encode(sx, sy);
-                            dirty = true;
-                            ++nc;
-                            if (nc > (int)NC) break;  // the reference returns from this cell
-                        }
-                    }
+        bool ok = true;
+        auto visit = [&](unsigned b, int sx, int sy) -> bool {
+            double4 xb = S.x[b];
+            double rb = xb.w;
+            V3 xab = mk3(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
+            xab = add3(xab, shift_vec(P, sx, sy));
+            double len = vlen<PREC>(xab);
+            double delta = len - (ra + rb);
+            if (delta < 0.0) {
+                unsigned b_orig = S.orig_of[b];
+                int cpos = pick_slot(mask, full, srow, B, t, b_orig, nc);
+                if (cpos >= (int)NC || nc + 1 > (int)NC) {
+                    raise_err(S.ctl, DERR_CAPACITY, (int)o);
+                    ok = false;
+                    return false;
                 }
-        // --- interact, history contacts ---
-        for (unsigned i = 0; i < NC; ++i) {
-            unsigned b_orig = srow[i * B + t];
-            if (b_orig == P.np) continue;  // empty slots already hold zero history
-            if (b_orig > P.np) { raise_err(S.ctl, DERR_CAPACITY, (int)o); return; }
-            size_t mempos = rowbase + i;
+                srow[cpos * B + t] = b_orig;
+                mask |= 1ull << cpos;
+                written |= 1ull << cpos;
+                S.dmcode[rowbase + cpos] = dm_encode(sx, sy);
+                ++nc;
+            }
+            return true;
+        };
+        if (cnt != NL_OVERFLOW) {
+            for (unsigned j = 0; j < cnt; ++j) {
+                uint32_t e = S.nl[(size_t)j * np + k];
+                uint32_t c = e >> 28;
+                int sx = (c & 1) ? 1 : ((c & 2) ? -1 : 0);
+                int sy = (c & 4) ? 1 : ((c & 8) ? -1 : 0);
+                if (!visit(e & 0x0fffffffu, sx, sy)) break;
+            }
+        } else {
+            for_each_cell_candidate(P, S, k, xa, visit);
+        }
+        if (!ok) return;
+        // --- interact, history contacts in slot order ---
+        uint64_t m = mask;
+        while (m) {
+            const int i = __ffsll((long long)m) - 1;
+            m &= m - 1;
+            const unsigned b_orig = srow[i * B + t];
+            if (b_orig >= P.np) { raise_err(S.ctl, DERR_CAPACITY, (int)o); return; }
+            const size_t mempos = rowbase + i;
             V3 dm = dm_decode(P, S.dmcode[mempos]);
             unsigned kb = S.pos_of[b_orig];
             double4 xb = S.x[kb];
@@ -278,48 +368,48 @@ __global__ void __launch_bounds__(128) k_contacts(DevParams P, DevState S)
                                                  S.delta_t[mempos], ra, rb, x_ab, len, delta_n);
                 S.delta_t[mempos] = make_double4(dt_new.x, dt_new.y, dt_new.z, 0.0);
             } else {
-                srow[i * B + t] = P.np;
-                dirty = true;
+                mask &= ~(1ull << i);
+                written |= 1ull << i;
                 S.delta_t[mempos] = make_double4(0.0, 0.0, 0.0, 0.0);
             }
         }
-        if (dirty)
-            for (unsigned i = 0; i < NC; ++i) S.contacts[rowbase + i] = srow[i * B + t];
+        if (written) {
+            uint64_t w = written;
+            while (w) {
+                int i = __ffsll((long long)w) - 1;
+                w &= w - 1;
+                S.contacts[rowbase + i] = (mask >> i) & 1ull ? srow[i * B + t] : P.np;
+            }
+            S.occ[o] = mask;
+        }
     } else if (MODEL == 1) {
         // findAndProcessContactsInCell, contactsearch.cuh:91-186
-        int gx, gy, gz;
-        grid_pos(P, xa, gx, gy, gz);
-        for (int dz = -1; dz < 2; ++dz)
-            for (int dy = -1; dy < 2; ++dy)
-                for (int dx = -1; dx < 2; ++dx) {
-                    int cx = gx + dx, cy = gy + dy, cz = gz + dz, sx, sy;
-                    if (!wrap_cell(P, cx, cy, cz, sx, sy)) continue;
-                    V3 dm = mk3(0.0f, 0.0f, 0.0f);
-                    if (sx > 0) dm = add3(dm, mk3(P.L[0], 0.0, 0.0));
-                    if (sx < 0) dm = sub3(dm, mk3(P.L[0], 0.0, 0.0));
-                    if (sy > 0) dm = add3(dm, mk3(0.0, P.L[1], 0.0));
-                    if (sy < 0) dm = sub3(dm, mk3(0.0, P.L[1], 0.0));
-                    unsigned cell = (unsigned)cx + (unsigned)cy * P.num[0] +
-                                    (P.num[0] * P.num[1]) * (unsigned)cz;
-                    unsigned start = S.cell_start[cell];
-                    if (start == 0xffffffffu) continue;
-                    unsigned end = S.cell_end[cell];
-                    for (unsigned b = start; b < end; ++b) {
-                        if (b == k) continue;
-                        double4 xb = S.x[b];
-                        double rb = xb.w;
-                        V3 x_ab = mk3(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
-                        x_ab = add3(x_ab, dm);
-                        double len = vlen<PREC>(x_ab);
-                        double delta_ab = len - (ra + rb);
-                        if (delta_ab < 0.0f)
-                            contact_linear_viscous<PREC>(P, F, T, p, vel_a, angvel_a, S.vel[b],
-                                                         xyz(S.angvel[b]), ra, rb, x_ab, len,
-                                                         delta_ab, P.kappa);
-                        else if (delta_ab < P.db)
-                            capillary_exp<PREC>(P, F, ra, rb, delta_ab, x_ab, len, P.kappa);
-                    }
-                }
+        auto visit = [&](unsigned b, int sx, int sy) -> bool {
+            double4 xb = S.x[b];
+            double rb = xb.w;
+            V3 x_ab = mk3(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z);
+            x_ab = add3(x_ab, shift_vec(P, sx, sy));
+            double len = vlen<PREC>(x_ab);
+            double delta_ab = len - (ra + rb);
+            if (delta_ab < 0.0f)
+                contact_linear_viscous<PREC>(P, F, T, p, vel_a, angvel_a, S.vel[b],
+                                             xyz(S.angvel[b]), ra, rb, x_ab, len, delta_ab,
+                                             P.kappa);
+            else if (delta_ab < P.db)
+                capillary_exp<PREC>(P, F, ra, rb, delta_ab, x_ab, len, P.kappa);
+            return true;
+        };
+        if (cnt != NL_OVERFLOW && !(P.db > 0.0 && P.kappa != 0.0)) {
+            for (unsigned j = 0; j < cnt; ++j) {
+                uint32_t e = S.nl[(size_t)j * np + k];
+                uint32_t c = e >> 28;
+                int sx = (c & 1) ? 1 : ((c & 2) ? -1 : 0);
+                int sy = (c & 4) ? 1 : ((c & 8) ? -1 : 0);
+                visit(e & 0x0fffffffu, sx, sy);
+            }
+        } else {
+            for_each_cell_candidate(P, S, k, xa, visit);
+        }
     }
 
     // --- walls (contactsearch.cuh:602-701) ---
@@ -367,6 +457,16 @@ __global__ void __launch_bounds__(128) k_contacts(DevParams P, DevState S)
     for (unsigned w = 0; w < P.nw && w < 5; ++w) S.walls_force_pp[o + (size_t)P.np * w] = wf[w];
 }
 
+// Occupancy masks of the slot rows (after the rows were set from the host).
+__global__ void k_occ_from_rows(DevParams P, DevState S)
+{
+    unsigned o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= P.np) return;
+    uint64_t m = 0;
+    for (unsigned i = 0; i < P.nc; ++i)
+        if (S.contacts[(size_t)o * P.nc + i] != P.np) m |= 1ull << i;
+    S.occ[o] = m;
+}
 // ---------------------------------------------------------------------
 // bondsLinear, src/cohesion.cuh:8-233: one thread per bond computes the
 // bond state; forces are added per particle in bond order (k_bond_gather)
@@ -663,6 +763,12 @@ __global__ void __launch_bounds__(256) k_integrate(DevParams P, DevState S)
     unsigned c = ((unsigned)iz * P.num[1]) * P.num[0] + (unsigned)iy * P.num[0] + (unsigned)ix;
     S.cell_new[k] = c;
     if (c != S.cell_of[k]) S.ctl->resort = 1;
+    // neighbour lists stay exact while every particle is within 0.45 skin
+    // of its position at the build
+    float4 xr = S.x_ref[k];
+    double ddx = x_new.x - (double)xr.x, ddy = x_new.y - (double)xr.y, ddz = x_new.z - (double)xr.z;
+    double lim = 0.45 * P.skin;
+    if (ddx * ddx + ddy * ddy + ddz * ddz > lim * lim) S.ctl->nl_rebuild = 1;
 }
 
 // Cell hash of the current positions (first step, after sph_set).
@@ -747,6 +853,7 @@ cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cud
 {
     if (P.np == 0) return cudaSuccess;
     const unsigned B = 128;
+    k_nl_build<<<blocks_for(P.np, B), B, 0, st>>>(P, S);
     size_t smem = (P.contactmodel == 2) ? (size_t)B * P.nc * sizeof(uint32_t) : 0;
     dim3 grid(blocks_for(P.np, B));
     if (P.contactmodel == 2) {
@@ -785,6 +892,13 @@ cudaError_t launch_integrate(const DevParams &P, const DevState &S, cudaStream_t
     }
     unsigned g = (P.nw > 0 && P.np > 0) ? P.nblocks256 : 1;
     k_walls_and_clock<<<g, 256, 0, st>>>(P, S);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_occ_from_rows(const DevParams &P, const DevState &S, cudaStream_t st)
+{
+    if (P.np == 0) return cudaSuccess;
+    k_occ_from_rows<<<blocks_for(P.np, 256), 256, 0, st>>>(P, S);
     return cudaGetLastError();
 }
 

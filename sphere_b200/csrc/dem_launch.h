@@ -15,6 +15,7 @@ cudaError_t launch_bonds(const DevParams &P, const DevState &S, int prec, double
 // shear-stress reduction (wmode 3), integration, wall reduction + wall
 // integration, loop counters
 cudaError_t launch_integrate(const DevParams &P, const DevState &S, cudaStream_t st);
+cudaError_t launch_occ_from_rows(const DevParams &P, const DevState &S, cudaStream_t st);
 cudaError_t launch_hash(const DevParams &P, const DevState &S, cudaStream_t st);
 // force = 1 sorts unconditionally; otherwise only when DevCtl::resort is set
 cudaError_t launch_resort(const DevParams &P, const DevState &S, unsigned char *scratch,

@@ -27,6 +27,12 @@ struct DevState {
     uint32_t *contacts;    // partner original index, np = empty
     uint8_t *dmcode;       // periodic shift of the slot (dm_encode)
     double4 *delta_t;      // tangential displacement (x, y, z, 0)
+    uint64_t *occ;         // occupied-slot bitmask per original index (nc <= 64)
+
+    // neighbour lists in sorted order: entry j of particle k at nl[j*np + k]
+    // = sorted index | periodic shift code << 28
+    uint32_t *nl, *nl_count;
+    float4 *x_ref;         // position at the last list build
 
     // walls
     double4 *wnx, *wmvfd;

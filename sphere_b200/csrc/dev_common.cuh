@@ -41,6 +41,8 @@ struct DevParams {
     double kappa, db, V_b;
     double sigma0_A, sigma0_f, tau_x;
     double lambda_bar, sigma_b, tau_b;
+    double skin;                   // neighbour-list skin [m]
+    uint32_t nlmax;                // neighbour-list entries per particle
 };
 
 // Loop state that lives on the device so captured graphs can replay steps.
@@ -56,7 +58,8 @@ struct DevCtl {
     unsigned barrier_count;    // grid barrier state
     unsigned barrier_gen;
     unsigned ticket;           // last-block-done counter
-    unsigned pad;
+    int nl_rebuild;            // 1: rebuild the neighbour lists before contacts
+    long long nl_builds;       // neighbour-list builds performed
 };
 
 struct V3 {

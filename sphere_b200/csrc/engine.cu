@@ -119,6 +119,11 @@ void Engine::build_params()
     p.kappa = h.kappa; p.db = h.db; p.V_b = h.V_b;
     p.sigma0_A = h.sigma0_A; p.sigma0_f = h.sigma0_f; p.tau_x = h.tau_x;
     p.lambda_bar = h.lambda_bar; p.sigma_b = h.sigma_b; p.tau_b = h.tau_b;
+    // neighbour-list skin: a tenth of the smallest radius
+    double rmin = 1e300;
+    for (uint32_t i = 0; i < h.np; ++i) rmin = std::min(rmin, h.x[i].w);
+    p.skin = h.np ? 0.1 * rmin : 0.0;
+    p.nlmax = nlmax;
 }
 
 int Engine::allocate_and_upload()
@@ -136,6 +141,10 @@ int Engine::allocate_and_upload()
     S.cell_start = dalloc<uint32_t>(h.ncells()); S.cell_end = dalloc<uint32_t>(h.ncells());
     S.contacts = dalloc<uint32_t>(slots); S.dmcode = dalloc<uint8_t>(slots);
     S.delta_t = dalloc<double4>(slots);
+    S.occ = dalloc<uint64_t>(n);
+    S.nl = dalloc<uint32_t>(n * (size_t)nlmax);
+    S.nl_count = dalloc<uint32_t>(n);
+    S.x_ref = dalloc<float4>(n);
     S.wnx = dalloc<double4>(6); S.wmvfd = dalloc<double4>(6); S.wacc = dalloc<double>(6);
     S.walls_force_pp = dalloc<double>(n * (h.nw ? h.nw : 1));
     S.tau_pp = dalloc<double>(n);
@@ -223,6 +232,7 @@ int Engine::allocate_and_upload()
     c.iter = 0;
     c.t_current = h.t_current;
     c.velocity_state = 1;
+    c.nl_rebuild = 1;
     up(S.ctl, &c, sizeof c);
     cudaError_t e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cuda_fail(e, "upload");
@@ -524,7 +534,10 @@ int Engine::set(int f, const void *src, size_t bytes)
         if (e == cudaSuccess) e = launch_sort_into(tmp, dst, S.orig_of, n, 8, stream);
     } else {
         switch (f) {
-        case SPH_F_CONTACTS: e = cudaMemcpyAsync(S.contacts, src, bytes, cudaMemcpyHostToDevice, stream); break;
+        case SPH_F_CONTACTS:
+            e = cudaMemcpyAsync(S.contacts, src, bytes, cudaMemcpyHostToDevice, stream);
+            if (e == cudaSuccess) e = launch_occ_from_rows(P, S, stream);
+            break;
         case SPH_F_DELTA_T: e = cudaMemcpyAsync(S.delta_t, src, bytes, cudaMemcpyHostToDevice, stream); break;
         case SPH_F_WALLS_NX: e = cudaMemcpyAsync(S.wnx, src, bytes, cudaMemcpyHostToDevice, stream); break;
         case SPH_F_WALLS_MVFD: e = cudaMemcpyAsync(S.wmvfd, src, bytes, cudaMemcpyHostToDevice, stream); break;
@@ -679,6 +692,10 @@ static int open_common(std::unique_ptr<Engine> &eng, const sph_opts *opts)
     e.precision = o.precision;
     e.integrator = o.integrator == 2 ? 2 : 3;
     e.capacity = o.contact_capacity > 0 ? (uint32_t)o.contact_capacity : 32;
+    if (e.capacity > 64)
+        return e.fail(sphb::ST_ARG, "contact_capacity above 64 slots is not supported");
+    if (e.hs.np >= (1u << 28))
+        return e.fail(sphb::ST_UNSUPPORTED, "more than 2^28 particles");
     e.verbose = o.verbose;
     e.graph_steps = o.graph_steps > 0 ? o.graph_steps : 64;
     e.warm_start = o.warm_start;

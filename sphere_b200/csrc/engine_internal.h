@@ -25,6 +25,7 @@ public:
     int precision = 0;
     int integrator = 3;
     uint32_t capacity = 32;
+    uint32_t nlmax = 48;          // neighbour-list entries per particle
     int verbose = 0;
     int graph_steps = 64;
     int warm_start = 0;

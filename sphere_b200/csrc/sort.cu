@@ -206,6 +206,7 @@ __global__ void __launch_bounds__(256) k_resort(DevParams P, DevState S, PermScr
     if (gtid == 0) {
         ctl->resort = 0;
         ctl->resorts += 1;
+        ctl->nl_rebuild = 1;   // sorted indices changed
     }
 }
 
