@@ -38,15 +38,16 @@ def _needs(obj: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build(verbose: bool = False, ptxas_info: bool = False, out: str = OUT,
+          build_dir: str = BUILD, defines=()) -> str:
+    os.makedirs(build_dir, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(HERE, "..", "include", "sphere_b200.h"))
     objs = []
     nv = nvcc()
     for src in SOURCES:
         path = os.path.join(CSRC, src)
-        obj = os.path.join(BUILD, src + ".o")
+        obj = os.path.join(build_dir, src + ".o")
         objs.append(obj)
         if not _needs(obj, [path, __file__] + headers):
             continue
@@ -55,17 +56,18 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
             cmd = [nv, "-x", "c++"] + COMMON + ["-c", path, "-o", obj]
         if src in NO_FMA:
             cmd.insert(1, "-fmad=false")
+        cmd += [f"-D{d}" for d in defines]
         if ptxas_info and src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
-    if _needs(OUT, objs):
-        cmd = [nv, "-shared"] + ARCH + ["-o", OUT] + objs + ["-lcuda"]
+    if _needs(out, objs):
+        cmd = [nv, "-shared"] + ARCH + ["-o", out] + objs + ["-lcuda"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
-    return OUT
+    return out
 
 
 if __name__ == "__main__":

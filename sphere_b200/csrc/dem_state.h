@@ -29,6 +29,10 @@ struct DevState {
     double4 *delta_t;      // tangential displacement (x, y, z, 0)
     uint64_t *occ;         // occupied-slot bitmask per original index (nc <= 64)
 
+    // mixed precision only (null otherwise): FP32 copies of the velocities
+    // in sorted order and FP32 tangential history per slot
+    float4 *vel_f, *angvel_f, *delta_t_f;
+
     // neighbour lists in sorted order: entry j of particle k at nl[j*np + k]
     // = sorted index | periodic shift code << 28
     uint32_t *nl, *nl_count;

@@ -142,6 +142,11 @@ int Engine::allocate_and_upload()
     S.contacts = dalloc<uint32_t>(slots); S.dmcode = dalloc<uint8_t>(slots);
     S.delta_t = dalloc<double4>(slots);
     S.occ = dalloc<uint64_t>(n);
+    if (precision == SPH_PREC_MIXED) {
+        S.vel_f = dalloc<float4>(n);
+        S.angvel_f = dalloc<float4>(n);
+        S.delta_t_f = dalloc<float4>(slots);
+    }
     S.nl = dalloc<uint32_t>(n * (size_t)nlmax);
     S.nl_count = dalloc<uint32_t>(n);
     S.x_ref = dalloc<float4>(n);
@@ -283,7 +288,9 @@ cudaError_t Engine::enqueue_stage(int stage)
     const int prec = precision == 0 ? 0 : 1;
     switch (stage) {
     case 0: return launch_resort(P, S, S.perm_scratch, 0, stream);
-    case 1: return launch_contacts(P, S, prec, stream);
+    case 1:
+        if (precision == SPH_PREC_MIXED) return launch_contacts_mixed(P, S, stream);
+        return launch_contacts(P, S, prec, stream);
     case 2: return launch_bonds(P, S, prec, bond_f, bond_t, stream);
     case 3: return enqueue_fluid();
     case 4: return launch_integrate(P, S, stream);
@@ -463,7 +470,10 @@ int Engine::get(int f, void *dst, size_t bytes)
         case SPH_F_CELLSTART: d2h(S.cell_start, (size_t)need); break;
         case SPH_F_CELLEND: d2h(S.cell_end, (size_t)need); break;
         case SPH_F_CONTACTS: d2h(S.contacts, (size_t)need); break;
-        case SPH_F_DELTA_T: d2h(S.delta_t, (size_t)need); break;
+        case SPH_F_DELTA_T:
+            if (S.delta_t_f) return get_delta_t_mixed((double *)dst);
+            d2h(S.delta_t, (size_t)need);
+            break;
         case SPH_F_DISTMOD: return get_distmod((double *)dst);
         case SPH_F_WALLS_NX: d2h(S.wnx, (size_t)need); break;
         case SPH_F_WALLS_MVFD: d2h(S.wmvfd, (size_t)need); break;
@@ -515,6 +525,19 @@ int Engine::get_distmod(double *dst)
     return ST_OK;
 }
 
+int Engine::get_delta_t_mixed(double *dst)
+{
+    size_t slots = (size_t)hs.np * capacity;
+    std::vector<float4> f(slots);
+    cudaError_t e = cudaMemcpyAsync(f.data(), S.delta_t_f, slots * 16, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "get");
+    for (size_t i = 0; i < slots; ++i) {
+        dst[4 * i] = f[i].x; dst[4 * i + 1] = f[i].y; dst[4 * i + 2] = f[i].z; dst[4 * i + 3] = 0.0;
+    }
+    return ST_OK;
+}
+
 int Engine::set(int f, const void *src, size_t bytes)
 {
     int64_t need = field_bytes(f);
@@ -538,11 +561,26 @@ int Engine::set(int f, const void *src, size_t bytes)
             e = cudaMemcpyAsync(S.contacts, src, bytes, cudaMemcpyHostToDevice, stream);
             if (e == cudaSuccess) e = launch_occ_from_rows(P, S, stream);
             break;
-        case SPH_F_DELTA_T: e = cudaMemcpyAsync(S.delta_t, src, bytes, cudaMemcpyHostToDevice, stream); break;
+        case SPH_F_DELTA_T:
+            if (S.delta_t_f) {
+                std::vector<float4> f(bytes / 32);
+                const double *d = (const double *)src;
+                for (size_t i = 0; i < f.size(); ++i)
+                    f[i] = make_float4((float)d[4 * i], (float)d[4 * i + 1], (float)d[4 * i + 2], 0.f);
+                e = cudaMemcpyAsync(S.delta_t_f, f.data(), f.size() * 16, cudaMemcpyHostToDevice, stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            } else {
+                e = cudaMemcpyAsync(S.delta_t, src, bytes, cudaMemcpyHostToDevice, stream);
+            }
+            break;
         case SPH_F_WALLS_NX: e = cudaMemcpyAsync(S.wnx, src, bytes, cudaMemcpyHostToDevice, stream); break;
         case SPH_F_WALLS_MVFD: e = cudaMemcpyAsync(S.wmvfd, src, bytes, cudaMemcpyHostToDevice, stream); break;
         default: return fail(ST_ARG, "field is read-only");
         }
+    }
+    if (e == cudaSuccess) {
+        static const int one = 1;
+        e = cudaMemcpyAsync(&S.ctl->nl_rebuild, &one, sizeof one, cudaMemcpyHostToDevice, stream);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cuda_fail(e, "set");

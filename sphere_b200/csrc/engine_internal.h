@@ -75,6 +75,7 @@ public:
     double *sorted_scalar(int f) const;
     int get(int f, void *dst, size_t bytes);
     int get_distmod(double *dst);
+    int get_delta_t_mixed(double *dst);
     int set(int f, const void *src, size_t bytes);
     int download_state();
     int write_bin(const char *path);
