@@ -756,6 +756,7 @@ static int one_step(orc_state *s)
         }
     }
     s->t_current += s->dt;
+    s->filetimeclock += s->dt;
     s->iter++;
     return s->err;
 }

@@ -62,6 +62,8 @@ struct orc_state {
     /* loop state */
     int64_t iter;
     int velocity_state;
+    double filetimeclock;   /* time since the last file output */
+    double host_wall0_w;    /* wall-0 position as of the last file output */
 
     /* options */
     int precision, integrator;

@@ -277,5 +277,8 @@ int orc_write_bin(orc_state *s, const char *path)
     }
     fwrite(s->color, 4, n, f);
     fclose(f);
+    /* a file output refreshes the host copy of the wall and the clock */
+    if (s->nw > 0) s->host_wall0_w = s->wnx[0].w;
+    s->filetimeclock = 0.0;
     return 0;
 }

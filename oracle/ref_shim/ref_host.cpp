@@ -37,6 +37,8 @@ unsigned int shared_data[1025];
 #include "cohesion.cuh"
 #include "contactsearch.cuh"
 #include "integration.cuh"
+#include "navierstokes.cuh"
+#include "darcy.cuh"
 
 template <class F> static void launch(unsigned grid, unsigned block, F f)
 {
@@ -49,6 +51,23 @@ template <class F> static void launch(unsigned grid, unsigned block, F f)
             f();
         }
     }
+}
+
+template <class F> static void launch3(dim3 grid, dim3 block, F f)
+{
+    ref_gridDim = grid;
+    ref_blockDim = block;
+    for (unsigned bz = 0; bz < grid.z; ++bz)
+        for (unsigned by = 0; by < grid.y; ++by)
+            for (unsigned bx = 0; bx < grid.x; ++bx) {
+                ref_blockIdx = make_uint3(bx, by, bz);
+                for (unsigned tz = 0; tz < block.z; ++tz)
+                    for (unsigned ty = 0; ty < block.y; ++ty)
+                        for (unsigned tx = 0; tx < block.x; ++tx) {
+                            ref_threadIdx = make_uint3(tx, ty, tz);
+                            f();
+                        }
+            }
 }
 
 static unsigned idiv_up(unsigned a, unsigned b) { return (a % b != 0) ? (a / b + 1) : (a / b); }
@@ -147,6 +166,7 @@ void DEM::transferToGlobalDeviceMemory(int)
     std::memcpy(dev_walls_nx, walls.nx, sizeof(Float4) * walls.nw);
     std::memcpy(dev_walls_mvfd, walls.mvfd, sizeof(Float4) * walls.nw);
     if (walls.nw) std::memcpy(dev_walls_tau_x, walls.tau_x, sizeof(Float));
+    if (fluid == 1 && cfd_solver == 1) transferDarcyToGlobalDeviceMemory(0);
 }
 
 void DEM::transferFromGlobalDeviceMemory()
@@ -171,16 +191,20 @@ void DEM::transferFromGlobalDeviceMemory()
     std::memcpy(e.p, dev_p, f1);
     std::memcpy(walls.nx, dev_walls_nx, sizeof(Float4) * walls.nw);
     std::memcpy(walls.mvfd, dev_walls_mvfd, sizeof(Float4) * walls.nw);
+    if (fluid == 1 && cfd_solver == 1) transferDarcyFromGlobalDeviceMemory(0);
 }
 
 void DEM::freeGlobalDeviceMemory() {}
-void DEM::initDarcyMemDev() { std::fprintf(stderr, "reference host build: Darcy not wired\n"); std::abort(); }
 
 /* ---- the step driver: DEM::startTime's loop body, dry part ---- */
 struct RefRun {
     DEM *dem;
     long iter;
     int velocity_state;
+    unsigned wall0_iz;
+    long nijac_last;
+    long nijac_total;
+    double filetimeclock;
 };
 
 /* summation (integration.cuh:309-341) uses a 256-wide shared-memory tree
@@ -199,6 +223,101 @@ static void ref_summation(const Float *in, Float *out, unsigned np, unsigned blo
         for (unsigned i = 128; i != 0; i /= 2)
             for (unsigned t = 0; t < i; ++t) cache[t] += cache[t + i];
         out[b] = cache[0];
+    }
+}
+
+
+/* The Darcy block of DEM::startTime, device.cu:1901-2426 (cfd_solver 1),
+ * kernels launched one thread at a time. */
+static void ref_darcy(RefRun *r)
+{
+    DEM &d = *r->dem;
+    unsigned np = d.np;
+    unsigned tpb = 256, bpg = idiv_up(np, tpb);
+    dim3 blk(8, 8, 8);
+    dim3 grd(idiv_up(d.grid.num[0], 8), idiv_up(d.grid.num[1], 8), idiv_up(d.grid.num[2], 8));
+    Darcy &D = d.darcy;
+    if (d.walls.nw > 0 && (d.walls.wmode[0] == 1 || d.walls.wmode[0] == 3))
+        r->wall0_iz = d.walls.nx->w / (d.grid.L[2] / d.grid.num[2]);
+    unsigned wall0_iz = r->wall0_iz;
+    auto ghost = [&](Float *f) {
+        launch3(grd, blk, [&] { setDarcyGhostNodes<Float>(f, D.bc_xn, D.bc_xp, D.bc_yn, D.bc_yp, D.bc_bot, D.bc_top); });
+    };
+    if (np > 0) {
+        ghost(d.dev_darcy_p);
+        launch3(grd, blk, [&] { findDarcyPressureGradient(d.dev_darcy_p, d.dev_darcy_grad_p); });
+        launch3(grd, blk, [&] { setDarcyGhostNodes<Float3>(d.dev_darcy_grad_p, D.bc_xn, D.bc_xp, D.bc_yn, D.bc_yp, D.bc_bot, D.bc_top); });
+        launch(bpg, tpb, [&] {
+            findDarcyPressureForceLinear(d.dev_x, d.dev_darcy_grad_p, d.dev_darcy_phi, wall0_iz,
+                                         D.rho_f, D.bc_top, d.dev_force, d.dev_darcy_f_p);
+        });
+    }
+    if ((r->iter % D.ndem) == 0) {
+        launch3(grd, blk, [&] {
+            findDarcyPorositiesLinear(d.dev_cellStart, d.dev_cellEnd, d.dev_x_sorted, d.dev_vel_sorted,
+                                      (unsigned)r->iter, D.ndem, np, D.c_phi, d.dev_darcy_phi,
+                                      d.dev_darcy_dphi, d.dev_darcy_div_v_p, d.dev_darcy_vp_avg);
+        });
+        if (d.grid.periodic == 2) {
+            launch3(grd, blk, [&] { copyDarcyPorositiesToEdges(d.dev_darcy_phi, d.dev_darcy_dphi, d.dev_darcy_div_v_p, d.dev_darcy_vp_avg); });
+            launch3(grd, blk, [&] { copyDarcyPorositiesToBottom(d.dev_darcy_phi, d.dev_darcy_dphi, d.dev_darcy_div_v_p, d.dev_darcy_vp_avg); });
+        }
+        if ((D.p_mod_A > 1.0e-5 || D.p_mod_A < -1.0e-5) && D.p_mod_f > 1.0e-7) {
+            Float new_pressure = D.p_top_orig + D.p_mod_A * sin(2.0 * M_PI * D.p_mod_f * d.time.current + D.p_mod_phi);
+            launch3(grd, blk, [&] { setDarcyTopPressure(new_pressure, d.dev_darcy_p, wall0_iz); });
+            launch3(grd, blk, [&] { setDarcyTopWallPressure(new_pressure, wall0_iz, d.dev_darcy_p); });
+        }
+        launch3(grd, blk, [&] { findDarcyPermeabilities(D.k_c, d.dev_darcy_phi, d.dev_darcy_k); });
+        ghost(d.dev_darcy_phi);
+        ghost(d.dev_darcy_k);
+        launch3(grd, blk, [&] { findDarcyPermeabilityGradients(d.dev_darcy_k, d.dev_darcy_grad_k); });
+        if (r->iter == 0) {
+            launch3(grd, blk, [&] { setDarcyNormZero(d.dev_darcy_norm); });
+            launch3(grd, blk, [&] { copyValues<Float>(d.dev_darcy_p, d.dev_darcy_p_old); });
+        }
+        auto flux = [&] {
+            launch3(grd, blk, [&] {
+                setDarcyGhostNodesFlux<Float>(d.dev_darcy_p, D.bc_bot, D.bc_top, D.bc_bot_flux,
+                                              D.bc_top_flux, d.dev_darcy_k, D.mu);
+            });
+        };
+        if (D.bc_bot == 4 || D.bc_top == 4) flux();
+        long done = 0;
+        for (unsigned int nijac = 0; nijac < D.maxiter; ++nijac) {
+            if (nijac == 0)
+                launch3(grd, blk, [&] { copyValues<Float>(d.dev_darcy_p, d.dev_darcy_p_old); });
+            ghost(d.dev_darcy_p);
+            if (nijac == 0)
+                launch3(grd, blk, [&] {
+                    firstDarcySolution(d.dev_darcy_p, d.dev_darcy_k, d.dev_darcy_phi, d.dev_darcy_dphi,
+                                       d.dev_darcy_div_v_p, d.dev_darcy_vp_avg, d.dev_darcy_grad_k,
+                                       D.beta_f, D.mu, D.bc_xn, D.bc_xp, D.bc_yn, D.bc_yp, D.bc_bot,
+                                       D.bc_top, D.ndem, wall0_iz, d.dev_darcy_p_constant,
+                                       d.dev_darcy_dp_expl);
+                });
+            launch3(grd, blk, [&] {
+                updateDarcySolution(d.dev_darcy_p_old, d.dev_darcy_dp_expl, d.dev_darcy_p, d.dev_darcy_k,
+                                    d.dev_darcy_phi, d.dev_darcy_dphi, d.dev_darcy_div_v_p,
+                                    d.dev_darcy_vp_avg, d.dev_darcy_grad_k, D.beta_f, D.mu, D.bc_xn,
+                                    D.bc_xp, D.bc_yn, D.bc_yp, D.bc_bot, D.bc_top, D.ndem, wall0_iz,
+                                    d.dev_darcy_p_constant, d.dev_darcy_p_new, d.dev_darcy_norm);
+            });
+            if (D.bc_top == 1) launch3(grd, blk, [&] { setDarcyTopWallFixedFlow(wall0_iz, d.dev_darcy_p); });
+            if (D.bc_bot == 4 || D.bc_top == 4) flux();
+            launch3(grd, blk, [&] { copyValues<Float>(d.dev_darcy_p_new, d.dev_darcy_p); });
+            done = nijac;
+            if (nijac % nijacnorm == 0) {
+                d.transferDarcyNormFromGlobalDeviceMemory();
+                double max_norm_res = d.maxNormResDarcy();
+                if (max_norm_res <= D.tolerance) break;
+            }
+        }
+        r->nijac_last = done;
+        r->nijac_total += done + 1;
+        if (r->filetimeclock + d.time.dt < d.time.file_dt)
+            launch3(grd, blk, [&] { setDarcyZeros<Float>(d.dev_darcy_dphi); });
+        ghost(d.dev_darcy_p);
+        launch3(grd, blk, [&] { findDarcyVelocities(d.dev_darcy_p, d.dev_darcy_phi, d.dev_darcy_k, D.mu, d.dev_darcy_v); });
     }
 }
 
@@ -250,6 +369,7 @@ static int ref_one_step(RefRun *r)
             });
         }
     }
+    if (d.fluid == 1 && d.cfd_solver == 1) ref_darcy(r);
     if (np > 0) {
         if (d.walls.nw > 0 && d.walls.wmode[0] == 3) {
             launch(bpg, tpb, [&] {
@@ -286,6 +406,7 @@ static int ref_one_step(RefRun *r)
         }
     }
     d.time.current += d.time.dt;
+    r->filetimeclock += d.time.dt;
     ++r->iter;
     return 0;
 }
@@ -297,7 +418,26 @@ void *ref_open(const char *path, int fluid)
     /* DEM(inputbin, verbosity, checkVals, dry, initCuda, transferConstMem,
      *     fluidFlow, device) -- sphere.h */
     DEM *d = new DEM(std::string(path), 0, 1, 0, 1, 1, fluid, 0);
-    RefRun *r = new RefRun{d, 0, 1};
+    RefRun *r = new RefRun{d, 0, 1, 10000000u, 0, 0, 0.0};
+    if (fluid && d->cfd_solver == 1) {
+        // deterministic ghost cells (the reference leaves them uninitialised)
+        unsigned nx = d->grid.num[0], ny = d->grid.num[1], nz = d->grid.num[2];
+        for (int z = -1; z <= (int)nz; ++z)
+            for (int y = -1; y <= (int)ny; ++y)
+                for (int x = -1; x <= (int)nx; ++x) {
+                    bool ghost = x < 0 || y < 0 || z < 0 || x == (int)nx || y == (int)ny || z == (int)nz;
+                    if (!ghost) continue;
+                    unsigned i = d->d_idx(x, y, z);
+                    d->dev_darcy_p[i] = 0.0;
+                    d->dev_darcy_phi[i] = 0.0;
+                    d->dev_darcy_dphi[i] = 0.0;
+                    d->dev_darcy_p_constant[i] = 0;
+                }
+        // device.cu:1017-1020
+        d->darcy.p_top_orig = d->darcy.p[d->d_idx(0, 0, d->darcy.nz - 1)] -
+                              d->darcy.p_mod_A * sin(2.0 * M_PI * d->darcy.p_mod_f * d->time.current +
+                                                     d->darcy.p_mod_phi);
+    }
     return r;
 }
 
@@ -309,7 +449,6 @@ int ref_step(void *h, long n)
         int rc = ref_one_step(r);
         if (rc) return rc;
     }
-    r->dem->transferFromGlobalDeviceMemory();
     return 0;
 }
 
@@ -355,6 +494,37 @@ long ref_get(void *h, const char *name, void *dst, size_t bytes)
     } else if (n == "bonds") { src = d.dev_bonds; need = 8 * (size_t)d.params.nb0; }
     else if (n == "bonds_delta") { src = d.dev_bonds_delta; need = 32 * (size_t)d.params.nb0; }
     else if (n == "bonds_omega") { src = d.dev_bonds_omega; need = 32 * (size_t)d.params.nb0; }
+    else if (n.rfind("darcy_", 0) == 0 && d.fluid == 1) {
+        unsigned nx = d.grid.num[0], ny = d.grid.num[1], nz = d.grid.num[2];
+        size_t nc = (size_t)nx * ny * nz;
+        static thread_local std::vector<double> buf;
+        if (n == "darcy_nijac_last" || n == "darcy_nijac_total") {
+            static thread_local long v;
+            v = n == "darcy_nijac_last" ? r->nijac_last : r->nijac_total;
+            src = &v; need = 8;
+        } else if (n == "darcy_f_p") {
+            src = d.dev_darcy_f_p; need = (size_t)np * 32;
+        } else {
+            const double *f = nullptr;
+            int comps = 1;
+            if (n == "darcy_p") f = d.dev_darcy_p;
+            else if (n == "darcy_phi") f = d.dev_darcy_phi;
+            else if (n == "darcy_dphi") f = d.dev_darcy_dphi;
+            else if (n == "darcy_k") f = d.dev_darcy_k;
+            else if (n == "darcy_norm") f = d.dev_darcy_norm;
+            else if (n == "darcy_v") { f = (const double *)d.dev_darcy_v; comps = 3; }
+            else if (n == "darcy_vp_avg") { f = (const double *)d.dev_darcy_vp_avg; comps = 3; }
+            else return -1;
+            buf.assign(nc * comps, 0.0);
+            for (unsigned z = 0; z < nz; ++z)
+                for (unsigned y = 0; y < ny; ++y)
+                    for (unsigned x = 0; x < nx; ++x)
+                        for (int c = 0; c < comps; ++c)
+                            buf[((size_t)(z * ny + y) * nx + x) * comps + c] =
+                                f[(size_t)d.d_idx(x, y, z) * comps + c];
+            src = buf.data(); need = buf.size() * 8;
+        }
+    }
     else return -1;
     if (!dst || bytes < need) return (long)need;
     std::memcpy(dst, src, need);

@@ -330,3 +330,34 @@ def shear_benchmark(n: int = 100000, seed: int = 1, sigma0: float = 20e3,
     d.time_total = 50000 * d.time_dt
     d.time_file_dt = d.time_total
     return d
+
+
+def init_fluid_darcy(d: BinData, mu: float = 8.9e-4, rho_f: float = 1.0e3, p: float = 0.0,
+                     k_c: float = 4.6e-10, beta_f: float = 4.5e-10, tolerance: float = 1.0e-3,
+                     maxiter: int = 10000, ndem: int = 1, bottom_no_flow: bool = False) -> None:
+    """``sim.initFluid(cfd_solver=1)`` (``python/sphere.py:3395-3508``):
+    Darcy arrays on the sorting grid, periodic sides, Dirichlet top and
+    bottom unless ``bottom_no_flow`` (``setFluidBottomNoFlow``, Neumann)."""
+    nx, ny, nz = (int(v) for v in d.num)
+    d.fluid = True
+    d.cfd_solver = 1
+    d.mu = mu
+    d.rho_f = rho_f
+    d.p_f = numpy.full((nx, ny, nz), p)
+    d.v_f = numpy.zeros((nx, ny, nz, 3))
+    d.phi = numpy.ones((nx, ny, nz))
+    d.dphi = numpy.zeros((nx, ny, nz))
+    d.p_mod_A = d.p_mod_f = d.p_mod_phi = 0.0
+    d.bc_xn = d.bc_xp = d.bc_yn = d.bc_yp = 2
+    d.bc_bot = 1 if bottom_no_flow else 0
+    d.bc_top = 0
+    d.free_slip_bot = d.free_slip_top = 1
+    d.bc_bot_flux = d.bc_top_flux = 0.0
+    d.p_f_constant = numpy.zeros((nx, ny, nz), dtype=numpy.int32)
+    d.tolerance = tolerance
+    d.maxiter = maxiter
+    d.ndem = ndem
+    d.c_phi = 1.0
+    d.f_p = numpy.zeros((d.np, 3))
+    d.beta_f = beta_f
+    d.k_c = k_c

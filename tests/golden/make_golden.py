@@ -45,8 +45,36 @@ def cases():
     yield "walls_nonperiodic", d
 
 
+DARCY_FIELDS = ("darcy_p", "darcy_phi", "darcy_k", "darcy_v", "darcy_f_p", "darcy_nijac_last",
+                "x", "vel", "force")
+
+
+def darcy_cases():
+    d = configs.settling_lattice(n=300, seed=15, nx=7, ny=7, nz=7, spacing=0.0195, steps=40)
+    configs.add_top_wall(d, 10e3)
+    d.w_x[0] -= 0.002
+    configs.init_fluid_darcy(d, mu=1.797e-6, k_c=3.5e-13, tolerance=1e-8, maxiter=2000,
+                             bottom_no_flow=True)
+    yield "darcy_consolidation", d
+
+
 def main():
     O.build(ref=True)
+    for name, d in darcy_cases():
+        path = os.path.join(HERE, f"{name}.bin")
+        binfile.write_bin(d, path)
+        ref = O.Reference(path, fluid=True)
+        out = {}
+        for s in (1, 2, 3):
+            ref.step(1)
+            for f in DARCY_FIELDS:
+                a = ref.get(f)
+                if f == "force":
+                    a = a[:, :3]
+                out[f"{f}@{s}"] = a
+        ref.close()
+        numpy.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print(name, "written")
     for name, d in cases():
         path = os.path.join(HERE, f"{name}.bin")
         binfile.write_bin(d, path)

@@ -23,7 +23,7 @@ def test_oracle_matches_reference_golden(case):
     gold = numpy.load(os.path.join(HERE, case + ".npz"))
     steps = sorted({int(k.split("@")[1]) for k in gold.files})
     fields = sorted({k.split("@")[0] for k in gold.files})
-    orc = O.Oracle(os.path.join(HERE, case + ".bin"))
+    orc = O.Oracle(os.path.join(HERE, case + ".bin"), fluid=case.startswith("darcy"))
     done = 0
     for s in steps:
         assert orc.step(s - done) == 0, orc.error()
@@ -33,6 +33,9 @@ def test_oracle_matches_reference_golden(case):
             if f in VEC3:
                 a = a[:, :3]
             b = gold[f"{f}@{s}"]
+            if f == "darcy_nijac_last":
+                a = a.astype(numpy.int64)
+                b = b.astype(numpy.int64)
             assert bits_equal(a, b), f"step {s}: " + diff_report(f, a, b)
     orc.close()
 
@@ -40,7 +43,7 @@ def test_oracle_matches_reference_golden(case):
 def test_golden_cases_have_contacts():
     for case in CASES:
         gold = numpy.load(os.path.join(HERE, case + ".npz"))
-        if case == "dense_model1":
+        if case in ("dense_model1", "darcy_consolidation"):
             continue
         n = gold["x@1"].shape[0]
         assert (gold["contacts@20"] != n).sum() > 50, case

@@ -90,3 +90,35 @@ def test_reference_fixture_init_1e4(tmp_path):
     bad = compare_states(orc.get, ref.get, FIELDS)
     assert not bad, bad
     assert (orc.get("contacts") != d.np).sum() > 10000
+
+
+DARCY_FIELDS = ("darcy_p", "darcy_phi", "darcy_dphi", "darcy_k", "darcy_v", "darcy_f_p",
+                "darcy_nijac_last", "force", "x", "vel")
+
+
+def darcy_case(seed, periodic=1, bottom_no_flow=True, top_wall=True, ndem=1):
+    d = configs.settling_lattice(n=300, seed=seed, nx=7, ny=7, nz=7, spacing=0.0195, steps=40)
+    d.periodic = periodic
+    if top_wall:
+        configs.add_top_wall(d, 10e3)
+        d.w_x[0] -= 0.002
+    configs.init_fluid_darcy(d, mu=1.797e-6, k_c=3.5e-13, tolerance=1e-8, maxiter=2000,
+                             bottom_no_flow=bottom_no_flow, ndem=ndem)
+    return d
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(bottom_no_flow=False), dict(periodic=2),
+                                dict(top_wall=False), dict(ndem=2)],
+                         ids=["neumann_bottom", "dirichlet_bottom", "periodic_x", "no_wall", "ndem2"])
+def test_darcy(tmp_path, kw):
+    d = darcy_case(51, **kw)
+    path = str(tmp_path / "darcy.bin")
+    binfile.write_bin(d, path)
+    orc = O.Oracle(path, fluid=True)
+    ref = O.Reference(path, fluid=True)
+    for _ in range(4):
+        assert orc.step(1) == 0, orc.error()
+        ref.step(1)
+        bad = compare_states(orc.get, ref.get, DARCY_FIELDS)
+        assert not bad, bad
+    assert orc.get("darcy_nijac_last")[0] > 10
