@@ -231,17 +231,18 @@ def _lattice(n: int, seed: int, r_min: float, r_max: float, gap: float = 0.02):
 
 
 def settle_packing(n: int = 100000, seed: int = 1, r_min: float = 0.008,
-                   r_max: float = 0.012, g_factor: float = 50.0, steps: int = 30000,
-                   quench_every: int = 500, precision: str = "mixed", log=None) -> BinData:
+                   r_max: float = 0.012, g_factor: float = 100.0,
+                   collapse_steps: int = 20000, quench_steps: int = 6000,
+                   quench_every: int = 1000, precision: str = "mixed", log=None) -> BinData:
     """A settled packing made by damped DEM settling on the GPU engine.
 
-    Spheres start on a jittered lattice and fall under g_factor * 9.81 m/s^2
-    with strong normal and tangential damping and a 5x time step; every
-    `quench_every` steps all velocities are set to zero, which drains the
-    kinetic energy the way packing generators usually do.  The last third
-    of the steps run at 1 g.  Used to make the dense starting state of the
-    shear workload (the 'prepacked by settling' step); it is not a timed
-    path.
+    Spheres start on a jittered lattice and collapse under g_factor * 9.81
+    m/s^2 with strong normal and tangential damping and a 5x time step
+    (collapse_steps); then the kinetic energy is drained by setting all
+    velocities to zero every quench_every steps, first at g_factor g and
+    then at 1 g (quench_steps each).  Used to make the dense starting state
+    of the shear workload (the 'prepacked by settling' step); it is not a
+    timed path.
     """
     from .engine import Engine  # the GPU engine
 
@@ -263,32 +264,35 @@ def settle_packing(n: int = 100000, seed: int = 1, r_min: float = 0.008,
     d.time_dt = 5.0 * time_step(d)
     d.time_total = 1e9
     d.time_file_dt = 1e9
+
+    def quench(eng, steps):
+        zero = numpy.zeros((n, 4))
+        for done in range(0, steps, quench_every):
+            eng.step(quench_every)
+            v = eng.get("vel")
+            vmax = float(numpy.sqrt((v[:, :3] ** 2).sum(axis=1)).max())
+            zero[:, 3] = v[:, 3]
+            eng.set("vel", zero)
+            eng.set("angvel", numpy.zeros((n, 4)))
+            if log:
+                log(f"settle: quench after {done + quench_every} steps, max |v| {vmax:.3e} m/s")
+
     eng = Engine(d, precision=precision, graph_steps=quench_every)
-    zero = numpy.zeros((n, 4))
-    done = 0
-    while done < steps:
-        if done == (2 * steps) // 3:
-            # last third at 1 g: reopen with the settled positions
-            xs = eng.get("x")
-            eng.close()
-            d.x = xs[:, :3].copy()
-            d.g = numpy.array([0.0, 0.0, -9.81])
-            eng = Engine(d, precision=precision, graph_steps=quench_every)
-        eng.step(quench_every)
-        done += quench_every
-        v = eng.get("vel")
-        vmax = float(numpy.sqrt((v[:, :3] ** 2).sum(axis=1)).max())
-        zero[:, 3] = v[:, 3]
-        eng.set("vel", zero)
-        eng.set("angvel", numpy.zeros((n, 4)))
-        if log and done % (10 * quench_every) == 0:
-            log(f"settle: {done} steps, max |v| before quench {vmax:.3e} m/s")
+    eng.step(collapse_steps)
+    quench(eng, quench_steps)
+    d.x = eng.get("x")[:, :3].copy()
+    eng.close()
+    d.g = numpy.array([0.0, 0.0, -9.81])
+    eng = Engine(d, precision=precision, graph_steps=quench_every)
+    quench(eng, quench_steps)
     state = d.copy()
     state.x = eng.get("x")[:, :3].copy()
+    c = eng.get("contacts")
+    if log:
+        log(f"settle: {float((c != n).sum()) / n:.2f} contacts per particle")
     eng.close()
     state.vel[:] = 0.0
     state.angvel[:] = 0.0
-    state.g = numpy.array([0.0, 0.0, -9.81])
     top = float(numpy.max(state.x[:, 2] + state.radius))
     state.L = state.L.copy()
     state.num = state.num.copy()
@@ -310,7 +314,7 @@ def shear_benchmark(n: int = 100000, seed: int = 1, sigma0: float = 20e3,
 
     cache_dir = cache_dir or os.environ.get("SPHB_CACHE", "/tmp/sphere_b200_cache")
     os.makedirs(cache_dir, exist_ok=True)
-    path = os.path.join(cache_dir, f"packing2_n{n}_seed{seed}.bin")
+    path = os.path.join(cache_dir, f"packing3_n{n}_seed{seed}.bin")
     if os.path.exists(path):
         base = read_bin(path)
     else:

@@ -177,9 +177,27 @@ __device__ double block_tree_sum(const double *in, unsigned np, unsigned nblocks
     return cache[0];
 }
 
+// Adds in[0..n) in index order (the reference's serial loop over block
+// partials, integration.cuh:67-68, 376-378).  All threads of the calling
+// block stage chunks in shared memory; thread 0 adds them one by one.
+__device__ double ordered_sum(const double *in, unsigned n, double *stage)
+{
+    double acc = 0.0;
+    for (unsigned base = 0; base < n; base += 2048) {
+        unsigned m = min(2048u, n - base);
+        __syncthreads();
+        for (unsigned i = threadIdx.x; i < m; i += blockDim.x) stage[i] = __ldcg(in + base + i);
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (unsigned i = 0; i < m; ++i) acc += stage[i];
+    }
+    return acc;
+}
+
 __global__ void __launch_bounds__(256) k_tau_partials(DevParams P, DevState S)
 {
     __shared__ double cache[256];
+    __shared__ double stage[2048];
     __shared__ bool last;
     if (S.ctl->err) return;
     double s = block_tree_sum(S.tau_pp, P.np, P.nblocks256, cache);
@@ -189,10 +207,11 @@ __global__ void __launch_bounds__(256) k_tau_partials(DevParams P, DevState S)
         last = atomicAdd(&S.ctl->ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        double tau = 0.0;
-        for (unsigned i = 0; i < P.nblocks256; ++i) tau += ((volatile double *)S.tau_partials)[i];
+    if (!last) return;
+    __threadfence();
+    double tau = 0.0;
+    tau = ordered_sum(S.tau_partials, P.nblocks256, stage);
+    if (threadIdx.x == 0) {
         S.ctl->tau_eff_x = tau;
         S.ctl->ticket = 0;
     }
@@ -377,6 +396,7 @@ __global__ void k_hash(DevParams P, DevState S)
 __global__ void __launch_bounds__(256) k_walls_and_clock(DevParams P, DevState S)
 {
     __shared__ double cache[256];
+    __shared__ double stage[2048];
     __shared__ bool last;
     DevCtl *ctl = S.ctl;
     if (ctl->err) return;
@@ -392,8 +412,11 @@ __global__ void __launch_bounds__(256) k_walls_and_clock(DevParams P, DevState S
         if (threadIdx.x == 0) last = true;
         __syncthreads();
     }
-    if (!last || threadIdx.x != 0) return;
+    if (!last) return;
     __threadfence();
+    // every wall sums the same (wall-0) partials, as the reference does
+    double wforce = P.nw > 0 ? ordered_sum(S.partials, P.nblocks256, stage) : 0.0;
+    if (threadIdx.x != 0) return;
     const long long iter = ctl->iter;
     const double t_current = ctl->t_current;
     const double dt = P.dt;
@@ -403,7 +426,7 @@ __global__ void __launch_bounds__(256) k_walls_and_clock(DevParams P, DevState S
         if (wmode == 0) continue;
         double acc0 = iter == 0 ? 0.0 : S.wacc[w];
         w_mvfd.z = 0.0;
-        for (unsigned b = 0; b < P.nblocks256; ++b) w_mvfd.z += ((volatile double *)S.partials)[b];
+        w_mvfd.z += wforce;
         double sigma_0 = w_mvfd.w + P.sigma0_A * sin(2.0 * SPHB_PI * P.sigma0_f * t_current);
         double N = -sigma_0 * P.L[0] * P.L[1];
         double acc = (w_mvfd.z + N) / w_mvfd.x;
