@@ -96,6 +96,8 @@ typedef enum sph_field {
     SPH_F_DARCY_F_P,    /* np x 4 doubles: pressure force on each particle */
     SPH_F_DARCY_ITERS,  /* 1 int64: Jacobi iterations of the last fluid step */
     SPH_F_DARCY_ITERS_TOTAL, /* 1 int64: Jacobi iterations since open */
+    SPH_F_DARCY_ITERS_EXACT, /* 1 int64: first iteration of the last solve whose
+                                residual met the tolerance (-1: none) */
     SPH_F_BONDS,        /* nb0 x 2 u32 */
     SPH_F_BONDS_DELTA,  /* nb0 x 4 doubles (t.x, t.y, t.z, n) */
     SPH_F_BONDS_OMEGA,
@@ -114,6 +116,11 @@ typedef struct sph_info {
 
 /* Fills *opts with the defaults (faithful FP64, TY3, 32 slots, device -1). */
 void sph_default_opts(sph_opts *opts);
+
+/* Reads and validates a .bin file without touching the device: the
+ * reference's `sphere --dry` (src/sphere.cpp:46-51: read, checkValues,
+ * report, exit).  The message of a failure is in sph_open_error(). */
+int sph_check_file(const char *bin_path, int fluid);
 
 /* Reads and validates a .bin file (src/file_io.cpp:30-417 +
  * src/sphere.cpp:145-345) and uploads the state.  Replaces `DEM dem(...)`

@@ -232,17 +232,21 @@ def _lattice(n: int, seed: int, r_min: float, r_max: float, gap: float = 0.02):
 
 def settle_packing(n: int = 100000, seed: int = 1, r_min: float = 0.008,
                    r_max: float = 0.012, g_factor: float = 100.0,
-                   collapse_steps: int = 20000, quench_steps: int = 6000,
+                   collapse_chunk: int = 5000, collapse_max: int = 200000,
+                   v_settled: float = 0.02, quench_steps: int = 6000,
                    quench_every: int = 1000, precision: str = "mixed", log=None) -> BinData:
     """A settled packing made by damped DEM settling on the GPU engine.
 
     Spheres start on a jittered lattice and collapse under g_factor * 9.81
-    m/s^2 with strong normal and tangential damping and a 5x time step
-    (collapse_steps); then the kinetic energy is drained by setting all
-    velocities to zero every quench_every steps, first at g_factor g and
-    then at 1 g (quench_steps each).  Used to make the dense starting state
-    of the shear workload (the 'prepacked by settling' step); it is not a
-    timed path.
+    m/s^2 with strong normal and tangential damping and a 5x time step, in
+    chunks of collapse_chunk steps until 99 % of the spheres are slower
+    than v_settled (at most collapse_max steps); the lattice must fall by about
+    half its height, which takes a few tens of milliseconds of model time.
+    Then the kinetic energy is drained by setting all velocities to zero
+    every quench_every steps, first at g_factor g and then at 1 g
+    (quench_steps each).  Used to make the dense starting state of the
+    shear workload (the 'prepacked by settling' step); it is not a timed
+    path.
     """
     from .engine import Engine  # the GPU engine
 
@@ -265,6 +269,12 @@ def settle_packing(n: int = 100000, seed: int = 1, r_min: float = 0.008,
     d.time_total = 1e9
     d.time_file_dt = 1e9
 
+    def v99_of(eng):
+        # 99th percentile speed: a few caged spheres rattle at 100 g long
+        # after the bulk has come to rest
+        v = eng.get("vel")
+        return float(numpy.percentile(numpy.sqrt((v[:, :3] ** 2).sum(axis=1)), 99.0))
+
     def quench(eng, steps):
         zero = numpy.zeros((n, 4))
         for done in range(0, steps, quench_every):
@@ -278,7 +288,15 @@ def settle_packing(n: int = 100000, seed: int = 1, r_min: float = 0.008,
                 log(f"settle: quench after {done + quench_every} steps, max |v| {vmax:.3e} m/s")
 
     eng = Engine(d, precision=precision, graph_steps=quench_every)
-    eng.step(collapse_steps)
+    done = 0
+    while done < collapse_max:
+        eng.step(collapse_chunk)
+        done += collapse_chunk
+        v99 = v99_of(eng)
+        if log:
+            log(f"settle: collapse {done} steps, 99th percentile |v| {v99:.3e} m/s")
+        if v99 < v_settled:
+            break
     quench(eng, quench_steps)
     d.x = eng.get("x")[:, :3].copy()
     eng.close()
@@ -314,7 +332,7 @@ def shear_benchmark(n: int = 100000, seed: int = 1, sigma0: float = 20e3,
 
     cache_dir = cache_dir or os.environ.get("SPHB_CACHE", "/tmp/sphere_b200_cache")
     os.makedirs(cache_dir, exist_ok=True)
-    path = os.path.join(cache_dir, f"packing3_n{n}_seed{seed}.bin")
+    path = os.path.join(cache_dir, f"packing4_n{n}_seed{seed}.bin")
     if os.path.exists(path):
         base = read_bin(path)
     else:

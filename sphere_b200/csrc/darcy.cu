@@ -1,20 +1,857 @@
-// Darcy porosity-coupled pressure solver (cfd_solver 1).
+// Darcy porosity-coupled pressure solver (cfd_solver 1) on the device.
+//
+// Follows the cfd_solver == 1 block of DEM::startTime
+// (src/device.cu:1901-2426) and the kernels of src/darcy.cuh, compiled with
+// -fmad=false like the reference.  Fields are ghost-padded
+// (nx+2)(ny+2)(nz+2) doubles (src/darcy.cpp:36-40).  The Jacobi fixed point
+// (firstDarcySolution + updateDarcySolution + copyValues, repeated) runs as
+// one cooperative kernel: ping-pong pressure buffers, each cell writes the
+// ghost faces that depend on it right after its update, the residual
+// maximum is reduced on the device every iteration, and the reference's
+// stopping rule (checked after iteration 0 and every 10th iteration) is
+// applied on the device -- no host round trip per check.
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "engine_internal.h"
+#include "dem_device.cuh"
 #include "../../include/sphere_b200.h"
 
 namespace sphb {
 
+struct DarcyParams {
+    int nx, ny, nz;
+    double dx, dy, dz;
+    double mu, rho_f, beta_f, k_c, c_phi, tolerance;
+    double p_mod_A, p_mod_f, p_mod_phi, p_top_orig;
+    double bc_bot_flux, bc_top_flux;
+    int bc_xn, bc_xp, bc_yn, bc_yp, bc_bot, bc_top;
+    unsigned maxiter, ndem;
+};
+
+struct DarcyCtl {
+    unsigned wall0_iz;             // from the host copy of the wall (file outputs)
+    long long nijac_last;          // the reference's nijac at the end of the solve
+    long long nijac_total;         // iterations performed since open
+    long long converged_at;        // first iteration whose residual met the tolerance
+    int converged;                 // 1: the last solve stopped at a residual check
+    unsigned long long res_bits[3];  // |residual| maxima as ordered bit patterns, 3-slot ring
+    int final_buf;                 // buffer holding the final pressure (0: p, 1: p2)
+    unsigned barrier_count, barrier_gen;
+    int err;
+};
+
+struct DarcyDev {
+    DarcyParams D;
+    size_t ng;
+    double *p, *p2, *p_old, *dp_expl, *phi, *dphi, *k, *div_v_p;
+    double *v, *vp_avg, *grad_p, *grad_k;  // 3 doubles per cell
+    int *p_constant;
+    double4 *f_p;                          // original particle order
+    double *gather;                        // nx*ny*nz*3 doubles for field reads
+    DarcyCtl *ctl;
+    double host_wall0_w;
+    long long conv_iters_last;
+};
+
+__device__ __forceinline__ unsigned didx(const DarcyParams &D, int x, int y, int z)
+{
+    return (unsigned)(x + 1) + ((unsigned)D.nx + 2u) * (unsigned)(y + 1) +
+           ((unsigned)D.nx + 2u) * ((unsigned)D.ny + 2u) * (unsigned)(z + 1);
+}
+
+__device__ __forceinline__ bool cell_of_thread(const DarcyParams &D, int &x, int &y, int &z)
+{
+    unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned n = (unsigned)D.nx * D.ny * D.nz;
+    if (i >= n) return false;
+    x = (int)(i % D.nx);
+    y = (int)((i / D.nx) % D.ny);
+    z = (int)(i / ((unsigned)D.nx * D.ny));
+    return true;
+}
+
+// setDarcyGhostNodes<T>, darcy.cuh:194-264 (comps doubles per cell)
+template <int C>
+__device__ __forceinline__ void ghost_from(const DarcyParams &D, double *f, int x, int y, int z,
+                                           const double *val)
+{
+    const int nx = D.nx, ny = D.ny, nz = D.nz;
+    auto put = [&](int X, int Y, int Z) {
+        double *d = &f[(size_t)C * didx(D, X, Y, Z)];
+        for (int c = 0; c < C; ++c) d[c] = val[c];
+    };
+    if (x == 0 && D.bc_xn == 0) put(-1, y, z);
+    if (x == 1 && D.bc_xn == 1) put(-1, y, z);
+    if (x == 0 && D.bc_xn == 2) put(nx, y, z);
+    if (x == nx - 1 && D.bc_xp == 0) put(nx, y, z);
+    if (x == nx - 2 && D.bc_xp == 1) put(nx, y, z);
+    if (x == nx - 1 && D.bc_xp == 2) put(-1, y, z);
+    if (y == 0 && D.bc_yn == 0) put(x, -1, z);
+    if (y == 1 && D.bc_yn == 1) put(x, -1, z);
+    if (y == 0 && D.bc_yn == 2) put(x, ny, z);
+    if (y == ny - 1 && D.bc_yp == 0) put(x, ny, z);
+    if (y == ny - 2 && D.bc_yp == 1) put(x, ny, z);
+    if (y == ny - 1 && D.bc_yp == 2) put(x, -1, z);
+    if (z == 0 && D.bc_bot == 0) put(x, y, -1);
+    if (z == 1 && D.bc_bot == 1) put(x, y, -1);
+    if (z == 0 && D.bc_bot == 2) put(x, y, nz);
+    if (z == nz - 1 && D.bc_top == 0) put(x, y, nz);
+    if (z == nz - 2 && D.bc_top == 1) put(x, y, nz);
+    if (z == nz - 1 && D.bc_top == 2) put(x, y, -1);
+}
+
+template <int C>
+__global__ void k_ghost(DarcyParams D, double *f)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    double val[C];
+    const double *s = &f[(size_t)C * didx(D, x, y, z)];
+    for (int c = 0; c < C; ++c) val[c] = s[c];
+    ghost_from<C>(D, f, x, y, z, val);
+}
+
+// flux ghost value below/above cell (x,y,z) from its pressure p
+// (setDarcyGhostNodesFlux, darcy.cuh:270-312)
+__device__ __forceinline__ void flux_ghost(const DarcyParams &D, const double *k, double *dst,
+                                           int x, int y, int z, double p)
+{
+    const double kk = k[didx(D, x, y, z)];
+    const double dz = D.dz;
+    double q_z = 0.;
+    if (z == 0) q_z = D.bc_bot_flux;
+    else if (z == D.nz - 1) q_z = D.bc_top_flux;
+    const double p_ghost = -D.mu / kk * q_z * dz + p;
+    if (z == 0 && D.bc_bot == 4) dst[didx(D, x, y, -1)] = p_ghost;
+    if (z == D.nz - 1 && D.bc_top == 4) dst[didx(D, x, y, D.nz)] = p_ghost;
+}
+
+// Inside the fused Jacobi loop the flux ghosts and the ordinary ghosts of
+// the next iterate are written in the same pass; the reference writes the
+// ordinary ghosts later (at the start of the next iteration), so where both
+// target one face (a periodic partner face) the ordinary ghost wins.
+__device__ __forceinline__ void flux_ghost_next(const DarcyParams &D, const double *k, double *dst,
+                                                int x, int y, int z, double p)
+{
+    const double kk = k[didx(D, x, y, z)];
+    double q_z = 0.;
+    if (z == 0) q_z = D.bc_bot_flux;
+    else if (z == D.nz - 1) q_z = D.bc_top_flux;
+    const double p_ghost = -D.mu / kk * q_z * D.dz + p;
+    if (z == 0 && D.bc_bot == 4 && D.bc_top != 2) dst[didx(D, x, y, -1)] = p_ghost;
+    if (z == D.nz - 1 && D.bc_top == 4 && D.bc_bot != 2) dst[didx(D, x, y, D.nz)] = p_ghost;
+}
+
+__global__ void k_flux_ghost(DarcyParams D, double *p, const double *k)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    flux_ghost(D, k, p, x, y, z, p[didx(D, x, y, z)]);
+}
+
+__global__ void k_copy_interior(DarcyParams D, const double *src, double *dst)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    unsigned c = didx(D, x, y, z);
+    dst[c] = src[c];
+}
+
+__global__ void k_zero_interior(DarcyParams D, double *f)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    f[didx(D, x, y, z)] = 0.0;
+}
+
+// findDarcyPressureGradient, darcy.cuh:889-943
+__global__ void k_pressure_gradient(DarcyParams D, const double *p, double *grad_p)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    double *g = &grad_p[3 * (size_t)didx(D, x, y, z)];
+    g[0] = (p[didx(D, x + 1, y, z)] - p[didx(D, x - 1, y, z)]) / (D.dx + D.dx);
+    g[1] = (p[didx(D, x, y + 1, z)] - p[didx(D, x, y - 1, z)]) / (D.dy + D.dy);
+    g[2] = (p[didx(D, x, y, z + 1)] - p[didx(D, x, y, z - 1)]) / (D.dz + D.dz);
+}
+
+__device__ __forceinline__ double sphere_volume(double r)
+{
+    // 4/3 pi r^3 with the reference's M_PI and pow (darcy.cuh:318-321)
+    return 4.0 / 3.0 * 3.14159265358979323846 * pow(r, 3.0);
+}
+
+__device__ __forceinline__ double weight_dist(V3 d, double dx, double dy, double dz)
+{
+    V3 a = mk3(fabs(d.x), fabs(d.y), fabs(d.z));
+    if (a.x < dx && a.y < dy && a.z < dz)
+        return (1.0 - a.x / dx) * (1.0 - a.y / dy) * (1.0 - a.z / dz);
+    return 0.0;
+}
+
+// findDarcyPressureForceLinear, darcy.cuh:948-1102 (one thread per particle
+// in sorted order; force[k] += f_p; f_p kept at the original index)
+__global__ void k_pressure_force(DevParams P, DevState S, DarcyParams D, const double *grad_p,
+                                 const DarcyCtl *dctl, double4 *f_p_out)
+{
+    unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (S.ctl->err || k >= P.np) return;
+    const unsigned nx = (unsigned)D.nx, ny = (unsigned)D.ny, nz = (unsigned)D.nz;
+    const double dx = D.dx, dy = D.dy, dz = D.dz;
+    const unsigned wall0_iz = dctl->wall0_iz;
+    double4 x = S.x[k];
+    unsigned i_x = (unsigned)floor((x.x - P.origo[0]) / (P.L[0] / P.num[0]));
+    unsigned i_y = (unsigned)floor((x.y - P.origo[1]) / (P.L[1] / P.num[1]));
+    unsigned i_z = (unsigned)floor((x.z - P.origo[2]) / (P.L[2] / P.num[2]));
+    if (i_x >= nx || i_y >= ny || i_z >= nz) {
+        // the 27 reads below would leave the padded grid
+        raise_err(S.ctl, DERR_OUTSIDE, (int)S.orig_of[k]);
+        return;
+    }
+    V3 X = mk3(i_x * dx + 0.5 * dx, i_y * dy + 0.5 * dy, i_z * dz + 0.5 * dz);
+    V3 gp = mk3(0., 0., 0.);
+    for (int d_iz = -1; d_iz < 2; d_iz++)
+        for (int d_iy = -1; d_iy < 2; d_iy++)
+            for (int d_ix = -1; d_ix < 2; d_ix++) {
+                int ix_n = (int)i_x + d_ix, iy_n = (int)i_y + d_iy, iz_n = (int)i_z + d_iz;
+                const double *gs = &grad_p[3 * (size_t)didx(D, ix_n, iy_n, iz_n)];
+                V3 g = mk3(gs[0], gs[1], gs[2]);
+                if ((ix_n == -1 && iy_n == -1) || (ix_n == -1 && iz_n == -1) ||
+                    (iy_n == -1 && iz_n == -1) || (ix_n == (int)nx && iy_n == (int)ny) ||
+                    (ix_n == (int)nx && iz_n == (int)nz) || (iy_n == (int)ny && iz_n == (int)nz) ||
+                    (ix_n == (int)nx && iy_n == -1) || (ix_n == (int)nx && iz_n == -1) ||
+                    (iy_n == (int)ny && ix_n == -1) || (iy_n == (int)ny && iz_n == -1) ||
+                    (iz_n == (int)nz && ix_n == -1) || (iz_n == (int)nz && iy_n == -1))
+                    g = mk3(0., 0., 0.);
+                // unsigned comparison, as in the reference
+                if (D.bc_top == 0 && i_z + (unsigned)d_iz >= wall0_iz - 1u) g.z = 0.0;
+                V3 n = mk3(dx * d_ix, dy * d_iy, dz * d_iz);
+                V3 xf = mk3(X.x + n.x, X.y + n.y, X.z + n.z);
+                double w = weight_dist(mk3(x.x - xf.x, x.y - xf.y, x.z - xf.z), dx, dy, dz);
+                gp = add3(gp, smul3(w, g));
+            }
+    const double v = sphere_volume(x.w);
+    const double rv = D.rho_f * v;
+    V3 f_p = mk3((-1.0 * gp.x) * v - rv * P.g[0], (-1.0 * gp.y) * v - rv * P.g[1],
+                 (-1.0 * gp.z) * v - rv * P.g[2]);
+    if (D.bc_top == 0 && i_z >= wall0_iz) f_p.z = 0.0;
+    double4 f = S.force[k];
+    f.x += f_p.x; f.y += f_p.y; f.z += f_p.z; f.w += 0.0;
+    S.force[k] = f;
+    f_p_out[S.orig_of[k]] = make_double4(f_p.x, f_p.y, f_p.z, 0.0);
+}
+
+// findDarcyPorositiesLinear, darcy.cuh:359-550
+__global__ void k_porosities(DevParams P, DevState S, DarcyParams D, double *phi_a, double *dphi_a,
+                             double *vp_avg)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    const unsigned cellidx = didx(D, x, y, z);
+    if (P.np == 0) {
+        phi_a[cellidx] = 0.9;
+        dphi_a[cellidx] = 0.0;
+        return;
+    }
+    const long long iter = S.ctl->iter;
+    const double dx = D.dx, dy = D.dy, dz = D.dz;
+    const V3 X = mk3(x * dx + 0.5 * dx, y * dy + 0.5 * dy, z * dz + 0.5 * dz);
+    double solid = 0.0, solid_new = 0.0, den = 0.0;
+    V3 num = mk3(0.0, 0.0, 0.0);
+    const double phi_0 = phi_a[cellidx];
+    for (int dzc = -1; dzc < 2; ++dzc)
+        for (int dyc = -1; dyc < 2; ++dyc)
+            for (int dxc = -1; dxc < 2; ++dxc) {
+                int cx = x + dxc, cy = y + dyc, cz = z + dzc, sx, sy;
+                if (cz == -1) cz = 1;
+                if (P.periodic == 2) {
+                    if (cy == -1) cy = 1;
+                    if (cy == (int)P.num[1]) cy = (int)P.num[1] - 2;
+                }
+                if (!wrap_cell(P, cx, cy, cz, sx, sy)) continue;
+                V3 dm = shift_vec(P, sx, sy);
+                unsigned cell = (unsigned)cx + (unsigned)cy * P.num[0] +
+                                (P.num[0] * P.num[1]) * (unsigned)cz;
+                unsigned start = S.cell_start[cell];
+                if (start == 0xffffffffu) continue;
+                unsigned end = S.cell_end[cell];
+                for (unsigned i = start; i < end; ++i) {
+                    double4 xr = S.x[i], v = S.vel[i];
+                    V3 dist = add3(mk3(X.x - xr.x, X.y - xr.y, X.z - xr.z), dm);
+                    double sw = weight_dist(dist, dx, dy, dz);
+                    double vol_p = sphere_volume(xr.w);
+                    solid += sw * vol_p;
+                    double sv = sw * vol_p;
+                    num = add3(num, mk3(sv * v.x, sv * v.y, sv * v.z));
+                    den += sw * vol_p;
+                    xr.x += v.x * P.dt; xr.y += v.y * P.dt; xr.z += v.z * P.dt;
+                    V3 d2 = add3(mk3(X.x - xr.x, X.y - xr.y, X.z - xr.z), dm);
+                    solid_new += weight_dist(d2, dx, dy, dz) * vol_p;
+                }
+            }
+    double cell_volume = dx * dy * dz;
+    if (z == D.nz - 1) cell_volume *= 0.875;
+    const double phi = fmin(0.9, fmax(0.1, 1.0 - solid / cell_volume));
+    const double phi_new = fmin(0.9, fmax(0.1, 1.0 - solid_new / cell_volume));
+    double dphi;
+    V3 vp = mk3(0.0, 0.0, 0.0);
+    if (iter == 0) {
+        dphi = 0.0;
+    } else {
+        dphi = 0.5 * (phi_new - phi_0);
+        vp = divs3(num, fmax(1.0e-16, den));
+    }
+    phi_a[cellidx] = phi * D.c_phi;
+    dphi_a[cellidx] = dphi * D.c_phi;
+    vp_avg[3 * (size_t)cellidx] = vp.x;
+    vp_avg[3 * (size_t)cellidx + 1] = vp.y;
+    vp_avg[3 * (size_t)cellidx + 2] = vp.z;
+}
+
+// copyDarcyPorositiesToEdges + ToBottom, darcy.cuh:556-628 (periodic == 2)
+__global__ void k_copy_edges(DarcyParams D, double *phi, double *dphi, double *div_v_p, double *vp)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    if (y == 0 || y == D.ny - 1) {
+        int yr = y == 0 ? 1 : D.ny - 2;
+        unsigned r = didx(D, x, yr, z), w = didx(D, x, y, z);
+        phi[w] = phi[r]; dphi[w] = dphi[r]; div_v_p[w] = div_v_p[r];
+        for (int c = 0; c < 3; ++c) vp[3 * (size_t)w + c] = vp[3 * (size_t)r + c];
+    }
+}
+
+__global__ void k_copy_bottom(DarcyParams D, double *phi, double *dphi, double *div_v_p, double *vp)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z) || z != 0) return;
+    unsigned r = didx(D, x, y, 1), w = didx(D, x, y, 0);
+    phi[w] = phi[r]; dphi[w] = dphi[r]; div_v_p[w] = div_v_p[r];
+    for (int c = 0; c < 3; ++c) vp[3 * (size_t)w + c] = vp[3 * (size_t)r + c];
+}
+
+// setDarcyTopPressure + setDarcyTopWallPressure (darcy.cuh:1195-1240) for
+// cells inside the grid
+__global__ void k_top_pressure(DarcyParams D, const DarcyCtl *dctl, double *p, double t)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    double np_ = D.p_top_orig + D.p_mod_A * sin(2.0 * 3.14159265358979323846 * D.p_mod_f * t + D.p_mod_phi);
+    if (z == D.nz - 1 || (unsigned)z == dctl->wall0_iz) p[didx(D, x, y, z)] = np_;
+    if (z == D.nz - 1 && dctl->wall0_iz == (unsigned)D.nz) p[didx(D, x, y, D.nz)] = np_;
+}
+
+// findDarcyPermeabilities, darcy.cuh:1266-1313
+__global__ void k_permeabilities(DarcyParams D, const double *phi, double *k)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    unsigned c = didx(D, x, y, z);
+    double ph = phi[c];
+    if (ph > 0.9999) ph = 0.9999;
+    double kk = D.k_c * pow(ph, 3.0) / pow(1.0 - ph, 2.0);
+    k[c] = fmin(2.7e-10, kk);
+}
+
+// findDarcyPermeabilityGradients, darcy.cuh:1316-1374
+__global__ void k_permeability_gradients(DarcyParams D, const double *k, double *grad_k)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    double *g = &grad_k[3 * (size_t)didx(D, x, y, z)];
+    g[0] = (k[didx(D, x + 1, y, z)] - k[didx(D, x - 1, y, z)]) / (D.dx + D.dx);
+    g[1] = (k[didx(D, x, y + 1, z)] - k[didx(D, x, y - 1, z)]) / (D.dy + D.dy);
+    g[2] = (k[didx(D, x, y, z + 1)] - k[didx(D, x, y, z - 1)]) / (D.dz + D.dz);
+}
+
+struct DarcyFields {
+    const double *phi, *dphi, *k, *vp_avg, *p_old, *dp_expl;
+    const int *p_constant;
+};
+
+// The pressure change of firstDarcySolution / updateDarcySolution
+// (darcy.cuh:1425-1598, 1602-1799) from the pressure field pf.
+__device__ __forceinline__ double dp_of(const DarcyParams &D, const DarcyFields &F, const double *pf,
+                                        unsigned wall0_iz, double dt, int x, int y, int z)
+{
+    const int nx = D.nx, ny = D.ny, nz = D.nz;
+    const double dx = D.dx, dy = D.dy, dz = D.dz;
+    const unsigned c = didx(D, x, y, z);
+    const double phi_xn = F.phi[didx(D, x - 1, y, z)], phi = F.phi[c];
+    const double phi_xp = F.phi[didx(D, x + 1, y, z)], phi_yn = F.phi[didx(D, x, y - 1, z)];
+    const double phi_yp = F.phi[didx(D, x, y + 1, z)], phi_zn = F.phi[didx(D, x, y, z - 1)];
+    const double phi_zp = F.phi[didx(D, x, y, z + 1)];
+    const double dphi = F.dphi[c];
+    const double *vp = &F.vp_avg[3 * (size_t)c];
+    const int p_constant = F.p_constant[c];
+    double p_xn = pf[didx(D, x - 1, y, z)];
+    const double p = pf[c];
+    double p_xp = pf[didx(D, x + 1, y, z)], p_yn = pf[didx(D, x, y - 1, z)];
+    double p_yp = pf[didx(D, x, y + 1, z)], p_zn = pf[didx(D, x, y, z - 1)];
+    double p_zp = pf[didx(D, x, y, z + 1)];
+    const double k_xn = F.k[didx(D, x - 1, y, z)], k = F.k[c], k_xp = F.k[didx(D, x + 1, y, z)];
+    const double k_yn = F.k[didx(D, x, y - 1, z)], k_yp = F.k[didx(D, x, y + 1, z)];
+    const double k_zn = F.k[didx(D, x, y, z - 1)], k_zp = F.k[didx(D, x, y, z + 1)];
+    if (x == 0 && D.bc_xn == 1) p_xn = p;
+    if (x == nx - 1 && D.bc_xp == 1) p_xp = p;
+    if (y == 0 && D.bc_yn == 1) p_yn = p;
+    if (y == ny - 1 && D.bc_yp == 1) p_yp = p;
+    if (z == 0 && D.bc_bot == 1) p_zn = p;
+    if (z == nz - 1 && D.bc_top == 1) p_zp = p;
+    const double gx = (phi_xp - phi_xn) / (dx + dx), gy = (phi_yp - phi_yn) / (dy + dy),
+                 gz = (phi_zp - phi_zn) / (dz + dz);
+    const double div_k_grad_p =
+        (2. * k_xp * k / (k_xp + k) * (p_xp - p) / dx - 2. * k_xn * k / (k_xn + k) * (p - p_xn) / dx) / dx +
+        (2. * k_yp * k / (k_yp + k) * (p_yp - p) / dy - 2. * k_yn * k / (k_yn + k) * (p - p_yn) / dy) / dy +
+        (2. * k_zp * k / (k_zp + k) * (p_zp - p) / dz - 2. * k_zn * k / (k_zn + k) * (p - p_zn) / dz) / dz;
+    const double ndt = D.ndem * dt;
+    double dp = ndt / (D.beta_f * phi * D.mu) * div_k_grad_p -
+                (ndt / (D.beta_f * phi * (1.0 - phi))) *
+                    (dphi / ndt + (vp[0] * gx + vp[1] * gy + vp[2] * gz));
+    if ((D.bc_bot == 0 && z == 0) || (D.bc_top == 0 && z == nz - 1) ||
+        ((unsigned)z >= wall0_iz && D.bc_top == 0) || (D.bc_xn == 0 && x == 0) ||
+        (D.bc_xp == 0 && x == nx - 1) || (D.bc_yn == 0 && y == 0) ||
+        (D.bc_yp == 0 && y == nx - 1) || p_constant == 1)
+        dp = 0.0;
+    return dp;
+}
+
+// firstDarcySolution: dp_expl from the current pressure
+__global__ void k_first_solution(DarcyParams D, DarcyFields F, const double *p, double *dp_expl,
+                                 const DarcyCtl *dctl, double dt)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    dp_expl[didx(D, x, y, z)] = dp_of(D, F, p, dctl->wall0_iz, dt, x, y, z);
+}
+
+// Bounded grid barrier for the cooperative Jacobi kernel.
+__device__ bool darcy_barrier(DarcyCtl *ctl, unsigned nblocks)
+{
+    __syncthreads();
+    __shared__ int ok;
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = &ctl->barrier_gen;
+        unsigned g = *gen;
+        __threadfence();
+        unsigned arrived = atomicAdd(&ctl->barrier_count, 1u);
+        ok = 1;
+        if (arrived == nblocks - 1) {
+            ctl->barrier_count = 0;
+            __threadfence();
+            atomicAdd(&ctl->barrier_gen, 1u);
+        } else {
+            unsigned spins = 0;
+            while (*gen == g) {
+                if (++spins > (1u << 24)) {
+                    atomicCAS(&ctl->err, 0, DERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                if (((volatile int *)&ctl->err)[0] == DERR_TIMEOUT) { ok = 0; break; }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// The Jacobi iterations of the reference (device.cu:2184-2386):
+// p_new = p_old + 0.5 dp_expl + 0.5 dp_impl(p); p_new <- 0.95 p + 0.05 p_new;
+// residual (p_new - p)/(p + 1e-16); stop when the maximum |residual| is at
+// most the tolerance at an iteration divisible by 10.
+__global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, double *pa, double *pb,
+                                                DarcyCtl *ctl, double dt, int exact_stop)
+{
+    __shared__ double wmax[8];
+    const unsigned G = gridDim.x;
+    const unsigned n = (unsigned)D.nx * D.ny * D.nz;
+    const unsigned stride = G * blockDim.x;
+    const unsigned wall0_iz = ctl->wall0_iz;
+    double *cur = pa, *nxt = pb;
+    long long nijac_done = 0;
+    long long converged_at = -1;
+    bool stop = false, conv = false;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->res_bits[0] = 0ull;
+        ctl->res_bits[1] = 0ull;
+        ctl->res_bits[2] = 0ull;
+    }
+    if (!darcy_barrier(ctl, G)) return;
+    for (unsigned nijac = 0; nijac < D.maxiter && !stop; ++nijac) {
+        double lmax = 0.0;
+        bool nan = false;
+        for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+            const int x = (int)(i % D.nx), y = (int)((i / D.nx) % D.ny),
+                      z = (int)(i / ((unsigned)D.nx * D.ny));
+            const unsigned c = didx(D, x, y, z);
+            const double dp_impl = dp_of(D, F, cur, wall0_iz, dt, x, y, z);
+            const double epsilon = 0.5, theta = 0.05;
+            const double p = cur[c];
+            double p_new = F.p_old[c] + (1.0 - epsilon) * F.dp_expl[c] + epsilon * dp_impl;
+            p_new = p * (1.0 - theta) + p_new * theta;
+            const double res = (p_new - p) / (p + 1.0e-16);
+            const double a = fabs(res);
+            if (a != a) nan = true;
+            else lmax = fmax(lmax, a);
+            nxt[c] = p_new;
+            // ghost faces of the next iterate that this cell determines
+            // (setDarcyGhostNodes at the start of the next iteration), and
+            // the flux ghosts, which the reference derives from the
+            // pressure before the copy
+            ghost_from<1>(D, nxt, x, y, z, &p_new);
+            if (D.bc_bot == 4 || D.bc_top == 4) flux_ghost_next(D, F.k, nxt, x, y, z, p);
+        }
+        // maximum over the grid: warp, block, then one atomic per block
+        for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+        if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = lmax;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double bm = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) bm = fmax(bm, wmax[w]);
+            atomicMax(&ctl->res_bits[nijac % 3], (unsigned long long)__double_as_longlong(bm));
+        }
+        if (__syncthreads_or(nan) && threadIdx.x == 0) atomicExch(&ctl->res_bits[nijac % 3], ~0ull);
+        if (!darcy_barrier(ctl, G)) return;
+        const unsigned long long bits = ((volatile unsigned long long *)ctl->res_bits)[nijac % 3];
+        // slot (nijac + 2) % 3 was last read before this barrier and is next
+        // written after the following one
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->res_bits[(nijac + 2) % 3] = 0ull;
+        nijac_done = nijac;
+        if (bits == ~0ull) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&ctl->err, 0, DERR_NAN);
+            stop = true;
+        } else {
+            const double m = __longlong_as_double((long long)bits);
+            if (m <= D.tolerance && converged_at < 0) converged_at = nijac;
+            if (m <= D.tolerance && (exact_stop || nijac % 10 == 0)) stop = conv = true;
+        }
+        double *t = cur;
+        cur = nxt;
+        nxt = t;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->nijac_last = nijac_done;
+        ctl->nijac_total += nijac_done + 1;
+        ctl->converged_at = converged_at;
+        ctl->converged = conv ? 1 : 0;
+        ctl->final_buf = cur == pa ? 0 : 1;
+    }
+}
+
+// findDarcyVelocities, darcy.cuh:1839-1897
+__global__ void k_velocities(DarcyParams D, const double *p, const double *phi, const double *k,
+                             double *v)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    unsigned c = didx(D, x, y, z);
+    double gx = (p[didx(D, x + 1, y, z)] - p[didx(D, x - 1, y, z)]) / (D.dx + D.dx);
+    double gy = (p[didx(D, x, y + 1, z)] - p[didx(D, x, y - 1, z)]) / (D.dy + D.dy);
+    double gz = (p[didx(D, x, y, z + 1)] - p[didx(D, x, y, z - 1)]) / (D.dz + D.dz);
+    double a = -k[c] / D.mu;
+    v[3 * (size_t)c] = (a * gx) / phi[c];
+    v[3 * (size_t)c + 1] = (a * gy) / phi[c];
+    v[3 * (size_t)c + 2] = (a * gz) / phi[c];
+}
+
+// Gathers interior cells (x fastest) of a padded field into dst.
+__global__ void k_gather_interior(DarcyParams D, const double *src, double *dst, int comps)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    size_t o = ((size_t)(z * D.ny + y) * D.nx + x) * comps;
+    for (int c = 0; c < comps; ++c) dst[o + c] = src[(size_t)didx(D, x, y, z) * comps + c];
+}
+
+// Copies the buffer holding the final pressure into p when it is the other one.
+__global__ void k_final_pressure(DarcyParams D, const DarcyCtl *ctl, double *p, const double *p2,
+                                 size_t ng)
+{
+    if (ctl->final_buf != 1) return;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < ng;
+         i += (size_t)gridDim.x * blockDim.x)
+        p[i] = p2[i];
+}
+
+// ---------------------------------------------------------------------
+// engine glue
+// ---------------------------------------------------------------------
+static unsigned cells_blocks(const DarcyParams &D) { return ((unsigned)D.nx * D.ny * D.nz + 255) / 256; }
+
 int Engine::darcy_init()
 {
     if (!hs.fluid) return ST_OK;
-    return fail(ST_UNSUPPORTED, "Darcy solver not built yet");
+    if (hs.cfd_solver != 1) return fail(ST_UNSUPPORTED, "only the Darcy solver (cfd_solver 1) is built");
+    if (hs.ndem == 0) return fail(ST_INPUT, "ndem must be positive");
+    darcy = new DarcyDev();
+    DarcyDev &Dd = *darcy;
+    DarcyParams &D = Dd.D;
+    D.nx = (int)hs.num[0]; D.ny = (int)hs.num[1]; D.nz = (int)hs.num[2];
+    D.dx = hs.L[0] / hs.num[0]; D.dy = hs.L[1] / hs.num[1]; D.dz = hs.L[2] / hs.num[2];
+    D.mu = hs.mu; D.rho_f = hs.rho_f; D.beta_f = hs.beta_f; D.k_c = hs.k_c; D.c_phi = hs.c_phi;
+    D.tolerance = hs.tolerance;
+    D.p_mod_A = hs.p_mod_A; D.p_mod_f = hs.p_mod_f; D.p_mod_phi = hs.p_mod_phi;
+    D.bc_bot_flux = hs.bc_bot_flux; D.bc_top_flux = hs.bc_top_flux;
+    D.bc_xn = hs.bc_xn; D.bc_xp = hs.bc_xp; D.bc_yn = hs.bc_yn; D.bc_yp = hs.bc_yp;
+    D.bc_bot = hs.bc_bot; D.bc_top = hs.bc_top;
+    D.maxiter = hs.maxiter; D.ndem = hs.ndem;
+    const size_t nx = D.nx, ny = D.ny, nz = D.nz;
+    const size_t ng = (nx + 2) * (ny + 2) * (nz + 2);
+    Dd.ng = ng;
+    auto didx_h = [&](size_t x, size_t y, size_t z) { return (x + 1) + (nx + 2) * (y + 1) + (nx + 2) * (ny + 2) * (z + 1); };
+    // device.cu:1017-1020
+    D.p_top_orig = hs.p_f[(nz - 1) * nx * ny] -
+                   hs.p_mod_A * sin(2.0 * 3.14159265358979323846 * hs.p_mod_f * hs.t_current + hs.p_mod_phi);
+    Dd.p = dalloc<double>(ng); Dd.p2 = dalloc<double>(ng); Dd.p_old = dalloc<double>(ng);
+    Dd.dp_expl = dalloc<double>(ng); Dd.phi = dalloc<double>(ng); Dd.dphi = dalloc<double>(ng);
+    Dd.k = dalloc<double>(ng); Dd.div_v_p = dalloc<double>(ng);
+    Dd.v = dalloc<double>(3 * ng); Dd.vp_avg = dalloc<double>(3 * ng);
+    Dd.grad_p = dalloc<double>(3 * ng); Dd.grad_k = dalloc<double>(3 * ng);
+    Dd.p_constant = dalloc<int>(ng);
+    Dd.f_p = dalloc<double4>(hs.np);
+    Dd.gather = dalloc<double>(3 * nx * ny * nz);
+    Dd.ctl = dalloc<DarcyCtl>(1);
+    if (!Dd.p || !Dd.p2 || !Dd.p_old || !Dd.dp_expl || !Dd.phi || !Dd.dphi || !Dd.k ||
+        !Dd.div_v_p || !Dd.v || !Dd.vp_avg || !Dd.grad_p || !Dd.grad_k || !Dd.p_constant ||
+        !Dd.f_p || !Dd.gather || !Dd.ctl) return fail(ST_CUDA, "device allocation failed (Darcy)");
+    std::vector<double> p(ng, 0.0), phi(ng, 0.0), dphi(ng, 0.0), v(3 * ng, 0.0);
+    std::vector<int> pc(ng, 0);
+    for (size_t z = 0; z < nz; ++z)
+        for (size_t y = 0; y < ny; ++y)
+            for (size_t x = 0; x < nx; ++x) {
+                size_t f = (z * ny + y) * nx + x, g = didx_h(x, y, z);
+                p[g] = hs.p_f[f]; phi[g] = hs.phi[f]; dphi[g] = hs.dphi[f];
+                pc[g] = hs.p_constant[f];
+                for (int c = 0; c < 3; ++c) v[3 * g + c] = hs.v_f[3 * f + c];
+            }
+    std::vector<double4> fp(hs.np);
+    for (uint32_t i = 0; i < hs.np; ++i) fp[i] = make_double4(hs.f_p[i].x, hs.f_p[i].y, hs.f_p[i].z, 0.0);
+    cudaMemcpyAsync(Dd.p, p.data(), ng * 8, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(Dd.phi, phi.data(), ng * 8, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(Dd.dphi, dphi.data(), ng * 8, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(Dd.v, v.data(), 3 * ng * 8, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(Dd.p_constant, pc.data(), ng * 4, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(Dd.f_p, fp.data(), hs.np * 32, cudaMemcpyHostToDevice, stream);
+    DarcyCtl c;
+    std::memset(&c, 0, sizeof c);
+    c.wall0_iz = 10000000u;
+    cudaMemcpyAsync(Dd.ctl, &c, sizeof c, cudaMemcpyHostToDevice, stream);
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "Darcy upload");
+    Dd.host_wall0_w = hs.nw > 0 ? hs.wnx[0].w : 0.0;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi, 256, 0);
+    if (per_sm < 1) return fail(ST_CUDA, "Jacobi kernel cannot be resident");
+    jacobi_grid = sms * (per_sm < 4 ? per_sm : 4);
+    unsigned need = cells_blocks(D);
+    if ((unsigned)jacobi_grid > need) jacobi_grid = (int)need;
+    return darcy_sync_wall();
 }
-int64_t Engine::darcy_field_bytes(int) const { return -1; }
-int Engine::darcy_get(int, void *, size_t) { return fail(ST_ARG, "unknown field"); }
-int Engine::darcy_download() { return ST_OK; }
-int Engine::step_with_fluid_log(uint64_t n) { return step(n); }
-cudaError_t Engine::enqueue_fluid() { return cudaSuccess; }
-void Engine::conv_open() {}
-void Engine::conv_close() {}
+
+// wall0_iz comes from the host's copy of wall 0, refreshed at file output
+// (device.cu:1908-1911 reads walls.nx->w on the host); it keeps its initial
+// value unless wall 0 moves under wmode 1 or 3.
+int Engine::darcy_sync_wall()
+{
+    if (!darcy) return ST_OK;
+    if (hs.nw > 0 && (hs.wmode[0] == 1 || hs.wmode[0] == 3))
+        darcy_wall0_iz = (unsigned)(darcy->host_wall0_w / (hs.L[2] / hs.num[2]));
+    cudaError_t e = cudaMemcpyAsync(&darcy->ctl->wall0_iz, &darcy_wall0_iz, 4, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    return e == cudaSuccess ? ST_OK : cuda_fail(e, "Darcy wall");
+}
+
+void Engine::darcy_set_host_wall()
+{
+    if (darcy) darcy->host_wall0_w = hs.nw > 0 ? hs.wnx[0].w : 0.0;
+}
+
+void Engine::darcy_free()
+{
+    delete darcy;   // device arrays are released with the engine's allocations
+    darcy = nullptr;
+}
+
+cudaError_t Engine::enqueue_fluid()
+{
+    if (!darcy) return cudaSuccess;
+    DarcyDev &Dd = *darcy;
+    const DarcyParams &D = Dd.D;
+    const unsigned cb = cells_blocks(D);
+    cudaError_t e;
+    if (hs.np > 0) {
+        k_ghost<1><<<cb, 256, 0, stream>>>(D, Dd.p);
+        k_pressure_gradient<<<cb, 256, 0, stream>>>(D, Dd.p, Dd.grad_p);
+        k_ghost<3><<<cb, 256, 0, stream>>>(D, Dd.grad_p);
+        k_pressure_force<<<(hs.np + 127) / 128, 128, 0, stream>>>(P, S, D, Dd.grad_p, Dd.ctl, Dd.f_p);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    // iter % ndem == 0, decided from the host's mirror of the step counter
+    if ((host_iter % (int64_t)D.ndem) != 0) return cudaSuccess;
+    k_porosities<<<cb, 256, 0, stream>>>(P, S, D, Dd.phi, Dd.dphi, Dd.vp_avg);
+    if (hs.periodic == 2) {
+        k_copy_edges<<<cb, 256, 0, stream>>>(D, Dd.phi, Dd.dphi, Dd.div_v_p, Dd.vp_avg);
+        k_copy_bottom<<<cb, 256, 0, stream>>>(D, Dd.phi, Dd.dphi, Dd.div_v_p, Dd.vp_avg);
+    }
+    if ((D.p_mod_A > 1.0e-5 || D.p_mod_A < -1.0e-5) && D.p_mod_f > 1.0e-7)
+        k_top_pressure<<<cb, 256, 0, stream>>>(D, Dd.ctl, Dd.p, host_t);
+    k_permeabilities<<<cb, 256, 0, stream>>>(D, Dd.phi, Dd.k);
+    k_ghost<1><<<cb, 256, 0, stream>>>(D, Dd.phi);
+    k_ghost<1><<<cb, 256, 0, stream>>>(D, Dd.k);
+    k_permeability_gradients<<<cb, 256, 0, stream>>>(D, Dd.k, Dd.grad_k);
+    const bool flux = D.bc_bot == 4 || D.bc_top == 4;
+    if (flux) k_flux_ghost<<<cb, 256, 0, stream>>>(D, Dd.p, Dd.k);
+    // nijac == 0: p -> p_old, ghosts, dp_expl
+    k_copy_interior<<<cb, 256, 0, stream>>>(D, Dd.p, Dd.p_old);
+    k_ghost<1><<<cb, 256, 0, stream>>>(D, Dd.p);
+    DarcyFields F{Dd.phi, Dd.dphi, Dd.k, Dd.vp_avg, Dd.p_old, Dd.dp_expl, Dd.p_constant};
+    k_first_solution<<<cb, 256, 0, stream>>>(D, F, Dd.p, Dd.dp_expl, Dd.ctl, P.dt);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // the second buffer starts as a copy (its ghost faces are read too)
+    if ((e = cudaMemcpyAsync(Dd.p2, Dd.p, Dd.ng * 8, cudaMemcpyDeviceToDevice, stream)) != cudaSuccess)
+        return e;
+    double dt = P.dt;
+    int exact = darcy_exact_stop;
+    void *args[] = {(void *)&D, (void *)&F, (void *)&Dd.p, (void *)&Dd.p2, (void *)&Dd.ctl,
+                    (void *)&dt, (void *)&exact};
+    e = cudaLaunchCooperativeKernel((void *)k_jacobi, dim3(jacobi_grid), dim3(256), args, 0, stream);
+    if (e != cudaSuccess) return e;
+    k_final_pressure<<<cb, 256, 0, stream>>>(D, Dd.ctl, Dd.p, Dd.p2, Dd.ng);
+    if (!darcy_keep_dphi) k_zero_interior<<<cb, 256, 0, stream>>>(D, Dd.dphi);
+    k_ghost<1><<<cb, 256, 0, stream>>>(D, Dd.p);
+    k_velocities<<<cb, 256, 0, stream>>>(D, Dd.p, Dd.phi, Dd.k, Dd.v);
+    return cudaGetLastError();
+}
+
+int64_t Engine::darcy_field_bytes(int f) const
+{
+    if (!darcy) return -1;
+    const size_t nc = (size_t)hs.num[0] * hs.num[1] * hs.num[2];
+    switch (f) {
+    case SPH_F_DARCY_P: case SPH_F_DARCY_PHI: case SPH_F_DARCY_DPHI: case SPH_F_DARCY_K:
+        return (int64_t)nc * 8;
+    case SPH_F_DARCY_V: return (int64_t)nc * 24;
+    case SPH_F_DARCY_F_P: return (int64_t)hs.np * 32;
+    case SPH_F_DARCY_ITERS: case SPH_F_DARCY_ITERS_TOTAL: case SPH_F_DARCY_ITERS_EXACT:
+        return 8;
+    default: return -1;
+    }
+}
+
+int Engine::darcy_get(int f, void *dst, size_t bytes)
+{
+    if (!darcy) return fail(ST_ARG, "no fluid in this run");
+    int64_t need = darcy_field_bytes(f);
+    if (need < 0) return fail(ST_ARG, "unknown field");
+    if (!dst || bytes < (size_t)need) return fail(ST_ARG, "destination buffer too small");
+    DarcyDev &Dd = *darcy;
+    const unsigned cb = cells_blocks(Dd.D);
+    cudaError_t e = cudaSuccess;
+    const double *src = nullptr;
+    int comps = 1;
+    switch (f) {
+    case SPH_F_DARCY_P: src = Dd.p; break;
+    case SPH_F_DARCY_PHI: src = Dd.phi; break;
+    case SPH_F_DARCY_DPHI: src = Dd.dphi; break;
+    case SPH_F_DARCY_K: src = Dd.k; break;
+    case SPH_F_DARCY_V: src = Dd.v; comps = 3; break;
+    case SPH_F_DARCY_F_P:
+        e = cudaMemcpyAsync(dst, Dd.f_p, (size_t)need, cudaMemcpyDeviceToHost, stream);
+        break;
+    default: {
+        DarcyCtl c;
+        e = cudaMemcpyAsync(&c, Dd.ctl, sizeof c, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "get");
+        long long v = f == SPH_F_DARCY_ITERS ? c.nijac_last
+                      : f == SPH_F_DARCY_ITERS_TOTAL ? c.nijac_total : c.converged_at;
+        std::memcpy(dst, &v, 8);
+        return ST_OK;
+    }
+    }
+    if (src) {
+        e = cudaSuccess;
+        k_gather_interior<<<cb, 256, 0, stream>>>(Dd.D, src, Dd.gather, comps);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dst, Dd.gather, (size_t)need, cudaMemcpyDeviceToHost, stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    return e == cudaSuccess ? ST_OK : cuda_fail(e, "get");
+}
+
+int Engine::darcy_download()
+{
+    if (!darcy) return ST_OK;
+    const size_t nc = hs.ncells();
+    int rc;
+    if ((rc = darcy_get(SPH_F_DARCY_P, hs.p_f.data(), nc * 8))) return rc;
+    if ((rc = darcy_get(SPH_F_DARCY_PHI, hs.phi.data(), nc * 8))) return rc;
+    if ((rc = darcy_get(SPH_F_DARCY_DPHI, hs.dphi.data(), nc * 8))) return rc;
+    if ((rc = darcy_get(SPH_F_DARCY_V, hs.v_f.data(), nc * 24))) return rc;
+    std::vector<double4> fp(hs.np);
+    if ((rc = darcy_get(SPH_F_DARCY_F_P, fp.data(), hs.np * 32))) return rc;
+    for (uint32_t i = 0; i < hs.np; ++i) hs.f_p[i] = d4{fp[i].x, fp[i].y, fp[i].z, 0.0};
+    return ST_OK;
+}
+
+void Engine::conv_open()
+{
+    if (!darcy) return;
+    std::string f = outdir + "/" + sid + "-conv.log";
+    convlog = std::fopen(f.c_str(), "w");
+}
+
+void Engine::conv_close()
+{
+    if (convlog) std::fclose(convlog);
+    convlog = nullptr;
+}
+
+// Dry runs step through the captured graphs; with fluid every step runs
+// eagerly because the Jacobi loop length is data dependent, and the
+// iteration count is read back for the conv log and the stopping check.
+int Engine::step_with_fluid_log(uint64_t n)
+{
+    if (!darcy) return step(n);
+    int warn = ST_OK;
+    for (uint64_t i = 0; i < n; ++i) {
+        const int64_t it = host_iter;
+        // dphi survives only the step that ends at a file output
+        // (device.cu:2400-2410)
+        darcy_keep_dphi = !(filetimeclock + hs.dt < hs.file_dt);
+        cudaError_t e = enqueue_step();
+        if (e != cudaSuccess) return cuda_fail(e, "step");
+        advance_host_clock(1);
+        warmed = true;
+        DarcyCtl c;
+        e = cudaMemcpyAsync(&c, darcy->ctl, sizeof c, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "step");
+        if (c.err == DERR_TIMEOUT) return fail(ST_TIMEOUT, "Darcy solver: a bounded device wait timed out");
+        if (c.err == DERR_NAN) return fail(ST_OUTSIDE, "Darcy solver: normalized residual is NaN");
+        const bool solved = (it % (int64_t)darcy->D.ndem) == 0;
+        // conv log lines as device.cu:2356-2372 (conv_log_interval 10)
+        if (solved) {
+            if (c.converged) {
+                if (convlog && it % 10 == 0)
+                    std::fprintf(convlog, "%lld\t%lld\n", (long long)it + 1, c.nijac_last);
+            } else {
+                warn = SPH_WARN_NOCONV;
+                if (convlog) std::fprintf(convlog, "%lld\t%lld\n", (long long)it + 1, c.nijac_last);
+            }
+        }
+        int rc = poll_errors("step");
+        if (rc) return rc;
+    }
+    return warn;
+}
 
 }  // namespace sphb

@@ -63,6 +63,8 @@ cudaError_t launch_sort_into(const void *src, void *dst, const uint32_t *orig_of
 // ---------------------------------------------------------------------
 Engine::~Engine()
 {
+    conv_close();
+    darcy_free();
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (void *p : allocations) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
@@ -81,15 +83,6 @@ int Engine::cuda_fail(cudaError_t e, const char *where)
     return ST_CUDA;
 }
 
-template <class T> T *Engine::dalloc(size_t n)
-{
-    void *p = nullptr;
-    size_t bytes = n ? n * sizeof(T) : sizeof(T);
-    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
-    cudaMemsetAsync(p, 0, bytes, stream);
-    allocations.push_back(p);
-    return (T *)p;
-}
 
 void Engine::build_params()
 {
@@ -399,6 +392,7 @@ void Engine::advance_host_clock(uint64_t n)
 {
     for (uint64_t i = 0; i < n; ++i) {
         host_t += hs.dt;
+        filetimeclock += hs.dt;
         ++host_iter;
     }
 }
@@ -635,10 +629,17 @@ int Engine::download_state()
     return rc;
 }
 
+// Writing a file also refreshes the host's copy of wall 0 that the Darcy
+// solver reads and restarts the file clock (device.cu:2556-2600).
 int Engine::write_bin(const char *path)
 {
     int rc = download_state();
     if (rc < 0) return rc;
+    filetimeclock = 0.0;
+    if (darcy) {
+        darcy_set_host_wall();
+        if ((rc = darcy_sync_wall()) < 0) return rc;
+    }
     return write_bin_file(path, hs, err);
 }
 
@@ -666,7 +667,6 @@ int Engine::run()
     if ((rc = write_status()) < 0) return rc;
     conv_open();
     double t = host_t;
-    double filetimeclock = 0.0;
     int warn = ST_OK;
     while (t <= hs.t_total) {
         // steps until the next file output or the end of the run
@@ -682,7 +682,6 @@ int Engine::run()
         if ((rc = step_with_fluid_log(n)) < 0) return rc;
         if (rc > 0) warn = rc;
         t = tt;
-        filetimeclock = fc;
         if (output) {
             hs.step_count += 1;
             std::snprintf(name, sizeof name, "%s/%s.output%05d.bin", outdir.c_str(), sid.c_str(),
@@ -690,7 +689,6 @@ int Engine::run()
             if ((rc = write_bin(name)) < 0) return rc;
             hs.t_current = t;
             if ((rc = write_status()) < 0) return rc;
-            filetimeclock = 0.0;
         }
         if (verbose)
             std::printf("\r  Current time: %g/%g s.      ", t, hs.t_total);
@@ -813,6 +811,21 @@ int sph_open_buffer(const void *bytes, size_t nbytes, const sph_opts *opts, cons
 }
 
 const char *sph_open_error(void) { return sphb::g_open_error.c_str(); }
+
+int sph_check_file(const char *bin_path, int fluid)
+{
+    if (!bin_path) return SPH_ERR_ARG;
+    sphb::HostState hs;
+    std::string err;
+    int rc = sphb::read_bin_file(bin_path, fluid, hs, err);
+    if (rc == 0 && hs.contactmodel != 1 && hs.contactmodel != 2 && hs.contactmodel != 3) {
+        err = "contact model not understood";
+        rc = SPH_ERR_INPUT;
+    }
+    if (rc == 0) rc = sphb::check_values(hs, err);
+    sphb::g_open_error = rc ? err : std::string();
+    return rc;
+}
 
 int sph_run(sph_engine *e) { return e ? e->e->run() : SPH_ERR_ARG; }
 

@@ -44,6 +44,7 @@ public:
     // loop state mirrored on the host (same double additions as the device)
     double host_t = 0.0;
     int64_t host_iter = 0;
+    double filetimeclock = 0.0;   // model time since the last file output
     DevCtl last_ctl{};
 
     cudaGraphExec_t graph_exec = nullptr;
@@ -55,6 +56,10 @@ public:
     DarcyDev *darcy = nullptr;
     MixedDev *mixed = nullptr;
     FILE *convlog = nullptr;
+    int jacobi_grid = 0;            // blocks of the cooperative Jacobi launch
+    int darcy_exact_stop = 0;       // 1: stop at the first converged iteration
+    bool darcy_keep_dphi = false;   // this step ends at a file output
+    unsigned darcy_wall0_iz = 10000000u;
 
     int fail(int code, const std::string &msg);
     int cuda_fail(cudaError_t e, const char *where);
@@ -84,6 +89,9 @@ public:
 
     // Darcy (cfd_solver 1); no-ops for dry runs
     int darcy_init();
+    int darcy_sync_wall();
+    void darcy_set_host_wall();
+    void darcy_free();
     int64_t darcy_field_bytes(int f) const;
     int darcy_get(int f, void *dst, size_t bytes);
     int darcy_download();
@@ -94,5 +102,16 @@ public:
     // mixed precision
     int mixed_init();
 };
+
+// Zero-filled device array owned by the engine (released in ~Engine).
+template <class T> T *Engine::dalloc(size_t n)
+{
+    void *p = nullptr;
+    size_t bytes = n ? n * sizeof(T) : sizeof(T);
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    cudaMemsetAsync(p, 0, bytes, stream);
+    allocations.push_back(p);
+    return (T *)p;
+}
 
 }  // namespace sphb

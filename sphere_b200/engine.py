@@ -23,14 +23,14 @@ FIELDS = [
     "es_dot", "es", "ev_dot", "ev", "p", "cellid", "index", "cellstart", "cellend",
     "contacts", "delta_t", "distmod", "walls_nx", "walls_mvfd", "walls_acc", "iter",
     "time", "darcy_p", "darcy_phi", "darcy_dphi", "darcy_k", "darcy_v", "darcy_f_p",
-    "darcy_iters", "darcy_iters_total", "bonds", "bonds_delta", "bonds_omega",
+    "darcy_iters", "darcy_iters_total", "darcy_iters_exact", "bonds", "bonds_delta", "bonds_omega",
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 _VEC4 = {"x", "vel", "angvel", "angpos", "force", "torque", "acc", "angacc", "xyzsum",
          "delta_t", "distmod", "walls_nx", "walls_mvfd", "darcy_f_p", "bonds_delta",
          "bonds_omega"}
 _U32 = {"cellid", "index", "cellstart", "cellend", "contacts", "bonds"}
-_I64 = {"iter", "darcy_iters", "darcy_iters_total"}
+_I64 = {"iter", "darcy_iters", "darcy_iters_total", "darcy_iters_exact"}
 
 STATUS = {
     0: "ok", 1: "Darcy solve did not converge", -1: "file error", -2: "version",
@@ -100,6 +100,8 @@ def lib() -> ctypes.CDLL:
     L.sph_last_error.argtypes = [P]
     L.sph_last_error.restype = ctypes.c_char_p
     L.sph_open_error.restype = ctypes.c_char_p
+    L.sph_check_file.argtypes = [ctypes.c_char_p, ctypes.c_int]
+    L.sph_check_file.restype = ctypes.c_int
     L.sph_close.argtypes = [P]
     L.sph_version.restype = ctypes.c_char_p
     _lib = L
@@ -223,3 +225,11 @@ class Engine:
 
     def write_bin(self, path) -> None:
         self._check(lib().sph_write_bin(self._h, os.fsencode(path)))
+
+
+def check_file(path, fluid=False):
+    """Reads and validates a .bin file without the device (``sphere --dry``).
+    Returns (status, message)."""
+    L = lib()
+    rc = L.sph_check_file(os.fsencode(path), int(bool(fluid)))
+    return rc, (L.sph_open_error().decode() if rc else "")

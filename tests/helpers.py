@@ -1,5 +1,13 @@
 """Shared helpers for the tests."""
+import os
+import sys
+import types
+
 import numpy
+import pytest
+
+# the reference's python tree, read-only; present only where it is mounted
+REF_PY = os.environ.get("SPHERE_REF_PY", "/root/reference/python")
 
 VEC3 = ("angvel", "angpos", "force", "torque", "xyzsum", "acc", "angacc")
 
@@ -57,3 +65,34 @@ def bonded_packing(configs, n=300, seed=21, spacing=0.0195, factor=1.05, max_bon
     d.tau_b = numpy.inf
     d.k_n = 1e7
     return d
+
+
+def import_reference_sphere():
+    """Imports python/sphere.py read-only with stand-ins for what it needs
+    but does not use here: matplotlib, and numpy.infty (NumPy 2)."""
+    if not os.path.isdir(REF_PY):
+        pytest.skip("reference python tree not present")
+    for m in ("matplotlib", "matplotlib.pyplot", "matplotlib.collections",
+              "matplotlib.colors", "matplotlib.cm", "matplotlib.patches",
+              "matplotlib.ticker", "matplotlib.font_manager"):
+        sys.modules.setdefault(m, types.ModuleType(m))
+    mpl = sys.modules["matplotlib"]
+    mpl.use = lambda *a, **k: None
+    mpl.rc = lambda *a, **k: None
+    mpl.rcParams = {}
+    sys.modules["matplotlib.font_manager"].FontProperties = object
+    if not hasattr(numpy, "infty"):
+        numpy.infty = numpy.inf
+    sys.path.insert(0, REF_PY)
+    try:
+        import sphere
+    finally:
+        sys.path.remove(REF_PY)
+    return sphere
+
+
+class Count(numpy.ndarray):
+    """1-element count arrays that work in range() (sphere.py predates NumPy 2)."""
+
+    def __index__(self):
+        return int(self[0])

@@ -11,7 +11,8 @@ import pytest
 
 from sphere_b200 import binfile, configs
 
-REF_PY = "/root/reference/python"
+from helpers import Count as _Count, import_reference_sphere as _import_reference_sphere
+
 REF_OUT = "/root/reference/output"
 
 
@@ -84,37 +85,6 @@ def test_reference_fixtures_upgrade(tmp_path, name, np_expected):
     assert numpy.array_equal(e.x, d.x) and numpy.array_equal(e.radius, d.radius)
     with pytest.raises(binfile.BinFormatError):
         binfile.read_bin(src)  # 2.11 is rejected like the reference does
-
-
-def _import_reference_sphere():
-    """Imports python/sphere.py read-only with stand-ins for what it needs
-    but does not use here: matplotlib, and numpy.infty (NumPy 2)."""
-    if not os.path.isdir(REF_PY):
-        pytest.skip("reference python tree not present")
-    for m in ("matplotlib", "matplotlib.pyplot", "matplotlib.collections",
-              "matplotlib.colors", "matplotlib.cm", "matplotlib.patches",
-              "matplotlib.ticker", "matplotlib.font_manager"):
-        sys.modules.setdefault(m, types.ModuleType(m))
-    mpl = sys.modules["matplotlib"]
-    mpl.use = lambda *a, **k: None
-    mpl.rc = lambda *a, **k: None
-    mpl.rcParams = {}
-    sys.modules["matplotlib.font_manager"].FontProperties = object
-    if not hasattr(numpy, "infty"):
-        numpy.infty = numpy.inf
-    sys.path.insert(0, REF_PY)
-    try:
-        import sphere
-    finally:
-        sys.path.remove(REF_PY)
-    return sphere
-
-
-class _Count(numpy.ndarray):
-    """1-element count arrays that work in range() (sphere.py predates NumPy 2)."""
-
-    def __index__(self):
-        return int(self[0])
 
 
 def test_writer_matches_reference_python_writer(tmp_path):
