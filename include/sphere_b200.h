@@ -56,6 +56,9 @@ typedef struct sph_opts {
     int warm_start;       /* Darcy: 0 previous-step guess, 1 learned warm start */
     int graph_steps;      /* DEM steps captured per CUDA graph launch; 0 = automatic */
     const char *output_dir; /* directory for .bin/status/conv outputs; NULL = "output" */
+    int step_kernel;      /* 0 automatic (the fused persistent step where it applies),
+                             1 per-stage kernels, 2 fused persistent step (error where
+                             it does not apply: bonds, fluid, wmode 3) */
 } sph_opts;
 
 /* Fields for sph_get/sph_set.  Vector fields use the reference's Float4
@@ -208,6 +211,54 @@ const char *sph_noalloc_error(void);
 
 /* Library build string: version, arch, compile flags of the DEM kernels. */
 const char *sph_version(void);
+
+/* ---------------------------------------------------------------------
+ * Batches: many independent boxes stepped by one launch of the fused
+ * persistent step kernel.  Every box is a dry simulation (no fluid, no
+ * bonds, no wmode-3 wall) with the same contact model and precision; boxes
+ * may differ in size, parameters, walls and time step.  This replaces
+ * running the reference binary once per box.
+ * --------------------------------------------------------------------- */
+typedef struct sph_batch sph_batch;
+
+typedef struct sph_batch_config {
+    int threads;     /* threads per block */
+    int group_size;  /* blocks that step one box together */
+    int grid;        /* blocks of the launch */
+    int tuned;       /* 1 after the autotuner ran */
+    int ntrials;     /* autotuner trials recorded */
+    int graph;       /* 1 when steps replay a captured CUDA graph */
+} sph_batch_config;
+
+typedef struct sph_batch_trial {
+    int threads, group_size, grid;
+    double ms_per_step;   /* device time of the trial launch per step */
+} sph_batch_trial;
+
+/* Opens nbox boxes from .bin files; opts applies to every box (fluid and
+ * step_kernel are ignored).  The message of a failure is in
+ * sph_batch_open_error(). */
+int sph_open_batch(const char *const *bin_paths, int nbox, const sph_opts *opts, sph_batch **out);
+int sph_open_batch_buffers(const void *const *bufs, const size_t *sizes, int nbox,
+                           const sph_opts *opts, sph_batch **out);
+const char *sph_batch_open_error(void);
+/* Advances every box by n steps.  The first call with at least 256 steps
+ * runs the autotuner on its first steps. */
+int sph_batch_step(sph_batch *b, uint64_t n);
+/* Same, without tuning; *device_ms = device time (CUDA events). */
+int sph_batch_step_timed(sph_batch *b, uint64_t n, double *device_ms);
+/* Times every (threads, group size) on trial_steps real steps each and
+ * keeps the fastest. */
+int sph_batch_autotune(sph_batch *b, uint64_t trial_steps);
+int sph_batch_size(sph_batch *b);
+int64_t sph_batch_field_bytes(sph_batch *b, int box, sph_field f);
+int sph_batch_get(sph_batch *b, int box, sph_field f, void *dst, size_t bytes);
+int sph_batch_write_bin(sph_batch *b, int box, const char *path);
+int sph_batch_get_config(sph_batch *b, sph_batch_config *cfg);
+/* Copies up to max autotuner trials; returns how many were recorded. */
+int sph_batch_get_trials(sph_batch *b, sph_batch_trial *out, int max);
+const char *sph_batch_last_error(sph_batch *b);
+void sph_batch_close(sph_batch *b);
 
 #ifdef __cplusplus
 }

@@ -6,6 +6,7 @@ compiled with -fmad=false so their arithmetic rounds like the reference's
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -19,9 +20,10 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 # kernels whose results must round exactly like the reference
-NO_FMA = {"dem_kernels.cu", "sort.cu", "darcy.cu"}
+NO_FMA = {"dem_kernels.cu", "sort.cu", "darcy.cu", "persistent_fp64.cu"}
 SOURCES = ["bin_io.cpp", "dem_kernels.cu", "sort.cu", "engine.cu", "darcy.cu", "dem_mixed.cu",
-           "noalloc_sort.cu"]
+           "noalloc_sort.cu", "engine_persist.cu", "persistent_fp64.cu", "persistent_mixed.cu",
+           "batch.cu"]
 
 
 def nvcc() -> str:
@@ -45,6 +47,7 @@ def build(verbose: bool = False, ptxas_info: bool = False, out: str = OUT,
     headers.append(os.path.join(HERE, "..", "include", "sphere_b200.h"))
     objs = []
     nv = nvcc()
+    jobs = []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(build_dir, src + ".o")
@@ -61,7 +64,11 @@ def build(verbose: bool = False, ptxas_info: bool = False, out: str = OUT,
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.check_call(cmd)
+        jobs.append(cmd)
+    # translation units compile independently
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(subprocess.check_call, c) for c in jobs]:
+            f.result()
     if _needs(out, objs):
         cmd = [nv, "-shared"] + ARCH + ["-o", out] + objs + ["-lcuda"]
         if verbose:

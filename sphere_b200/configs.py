@@ -383,3 +383,73 @@ def init_fluid_darcy(d: BinData, mu: float = 8.9e-4, rho_f: float = 1.0e3, p: fl
     d.f_p = numpy.zeros((d.np, 3))
     d.beta_f = beta_f
     d.k_c = k_c
+
+
+def _fcc_positions(n: int, d_nn: float, z0: float):
+    """First n sites of a face-centred cubic lattice with nearest-neighbour
+    distance d_nn, filled layer by layer from z0 upward in a square periodic
+    cross-section; returns (x, nx_cells, a)."""
+    a = d_nn * math.sqrt(2.0)
+    nxc = max(2, int(math.ceil((n / 4.0) ** (1.0 / 3.0))))
+    basis = numpy.array([[0.0, 0.0, 0.0], [0.5, 0.5, 0.0], [0.5, 0.0, 0.5], [0.0, 0.5, 0.5]])
+    nzc = int(math.ceil(n / (4.0 * nxc * nxc))) + 1
+    iz, iy, ix = numpy.meshgrid(numpy.arange(nzc), numpy.arange(nxc), numpy.arange(nxc),
+                                indexing="ij")
+    cells = numpy.stack([ix.ravel(), iy.ravel(), iz.ravel()], axis=1).astype(numpy.float64)
+    sites = (cells[:, None, :] + basis[None, :, :]).reshape(-1, 3) * a
+    # fill by height (stable: equal heights keep lattice order)
+    order = numpy.argsort(sites[:, 2], kind="stable")
+    x = sites[order[:n]].copy()
+    x[:, 2] += z0
+    return x, nxc, a
+
+
+def fcc_shear_box(n: int, seed: int, r_min: float = 0.009, r_max: float = 0.011,
+                  sigma0: float = 20e3, shear_velocity: float = 1e-4, mu: float = 0.5,
+                  k_n: float = 1.16e7, contactmodel: int = 2) -> BinData:
+    """One shear box of the batched ensemble: n spheres (radii U(r_min,
+    r_max)) on a face-centred cubic lattice whose nearest neighbours are
+    2.002 r_max apart (a dense start without settling), periodic x/y, the
+    sphere defaults with k_n = k_t, friction mu, gravity, then ``sim.shear``:
+    fixed bottom layer, top layer at shear_velocity, a top wall at normal
+    stress sigma0."""
+    rng = numpy.random.default_rng(seed)
+    d = BinData()
+    _particles(d, n)
+    d.radius = rng.uniform(r_min, r_max, size=n)
+    x, nxc, a = _fcc_positions(n, 2.0 * r_max * 1.001, r_max * 1.001)
+    d.x = x
+    default_params(d, mu_s=mu, mu_d=mu, k_n=k_n, k_t=k_n)
+    d.contactmodel = contactmodel
+    d.g = numpy.array([0.0, 0.0, -9.81])
+    side = nxc * a
+    ncell = max(3, int(math.floor(side / (2.1 * r_max))))
+    cell = side / ncell
+    top = float(numpy.max(d.x[:, 2] + d.radius))
+    nz = max(3, int(math.ceil(top * 1.05 / cell)))
+    grid_for(d, L=[side, side, nz * cell], dx=cell)
+    d.periodic = 1
+    d.nw = 0
+    init_temporal(d, total=1.0, file_dt=1.0)
+    shear_setup(d, shear_velocity, sigma0)
+    return d
+
+
+def batch_shear_boxes(nbox: int = 256, seed: int = 7, n_min: int = 2000, n_max: int = 20000,
+                      scale: float = 1.0):
+    """The batched ensemble: nbox independent shear boxes with particle
+    counts log-uniform in [n_min, n_max] (times scale), radii U(0.009,
+    0.011) m, sigma0 from {10, 20, 40, 80, 160} kPa, shear velocity
+    U(1e-5, 1e-3) m/s, k_n = k_t = 1.16e7 N/m, mu U(0.3, 0.6).  Returns
+    (boxes, meta) with the drawn parameters per box."""
+    rng = numpy.random.default_rng(seed)
+    boxes, meta = [], []
+    for b in range(nbox):
+        n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max))) * scale))
+        n = max(n, 32)
+        sigma0 = float(rng.choice([10e3, 20e3, 40e3, 80e3, 160e3]))
+        vs = float(rng.uniform(1e-5, 1e-3))
+        mu = float(rng.uniform(0.3, 0.6))
+        boxes.append(fcc_shear_box(n, seed * 100003 + b, sigma0=sigma0, shear_velocity=vs, mu=mu))
+        meta.append({"n": n, "sigma0": sigma0, "shear_velocity": vs, "mu": mu})
+    return boxes, meta

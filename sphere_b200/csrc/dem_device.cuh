@@ -378,22 +378,25 @@ __device__ __forceinline__ int pick_slot(uint64_t mask, uint64_t full, const uin
     return nc;
 }
 
+// Results of the contact search and force evaluation of one particle.
+struct ContactOut {
+    V3 F, T;
+    double es_dot, ev_dot, p;
+    double wf[5];   // force on each dynamic wall (walls_force_pp)
+};
+
+// Contact search + forces of sorted particle k (topology and interact of
+// the reference, walls included).  srow is the thread's slot-row scratch in
+// shared memory (entry i at srow[i * B + t]).  Returns false after raising
+// a capacity error.
 // PREC 0: faithful FP64, 1: FP64, 2: mixed (FP64 overlap, FP32 contact law,
 // FP64 accumulation).
-// 6 resident blocks of 128 threads per SM (80 registers): measured best
-// between 1 and 8 on the dense-shear workload.
-#ifndef SPHB_CONTACT_MINB
-#define SPHB_CONTACT_MINB 6
-#endif
 template <int PREC, int MODEL>
-__global__ void __launch_bounds__(128, SPHB_CONTACT_MINB) k_contacts(DevParams P, DevState S)
+__device__ __forceinline__ bool contact_particle(const DevParams &P, const DevState &S, unsigned k,
+                                                 uint32_t *srow, unsigned B, unsigned t,
+                                                 ContactOut &out)
 {
     constexpr int TP = PREC == 2 ? 1 : PREC;  // precision of overlap tests
-    extern __shared__ uint32_t srow[];
-    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k == 0 && S.ctl->nl_rebuild) S.ctl->nl_rebuild = 0;  // k_nl_build has run
-    if (S.ctl->err || k >= P.np) return;
-    const unsigned B = blockDim.x, t = threadIdx.x;
     const unsigned NC = P.nc;
     const uint64_t full = NC >= 64 ? ~0ull : ((1ull << NC) - 1ull);
     const unsigned o = S.orig_of[k];
@@ -455,14 +458,14 @@ __global__ void __launch_bounds__(128, SPHB_CONTACT_MINB) k_contacts(DevParams P
         } else {
             for_each_cell_candidate(P, S, k, xa, visit);
         }
-        if (!ok) return;
+        if (!ok) return false;
         // --- interact, history contacts in slot order ---
         uint64_t m = mask;
         while (m) {
             const int i = __ffsll((long long)m) - 1;
             m &= m - 1;
             const unsigned b_orig = srow[i * B + t];
-            if (b_orig >= P.np) { raise_err(S.ctl, DERR_CAPACITY, (int)o); return; }
+            if (b_orig >= P.np) { raise_err(S.ctl, DERR_CAPACITY, (int)o); return false; }
             const size_t mempos = rowbase + i;
             V3 dm = dm_decode(P, S.dmcode[mempos]);
             unsigned kb = S.pos_of[b_orig];
@@ -563,16 +566,242 @@ __global__ void __launch_bounds__(128, SPHB_CONTACT_MINB) k_contacts(DevParams P
         if (dw < 0.0f)
             wf[4] = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx[4]), dw, wvel[4]);
     }
-    // --- write-back (contactsearch.cuh:706-724) ---
-    S.force[k] = make_double4(F.x, F.y, F.z, 0.0f);
-    S.torque[k] = make_double4(T.x, T.y, T.z, 0.0f);
-    S.es_dot[k] = es_dot;
-    S.ev_dot[k] = ev_dot;
-    S.es[k] += es_dot * P.dt;
-    S.ev[k] += ev_dot * P.dt;
-    S.p[k] = p;
-    for (unsigned w = 0; w < P.nw && w < 5; ++w) S.walls_force_pp[o + (size_t)P.np * w] = wf[w];
+    out.F = F;
+    out.T = T;
+    out.es_dot = es_dot;
+    out.ev_dot = ev_dot;
+    out.p = p;
+    for (int w = 0; w < 5; ++w) out.wf[w] = wf[w];
+    return true;
 }
 
+// Write-back of one particle's contact results (contactsearch.cuh:706-724).
+__device__ __forceinline__ void contact_writeback(const DevParams &P, const DevState &S, unsigned k,
+                                                  const ContactOut &c)
+{
+    const unsigned o = S.orig_of[k];
+    S.force[k] = make_double4(c.F.x, c.F.y, c.F.z, 0.0f);
+    S.torque[k] = make_double4(c.T.x, c.T.y, c.T.z, 0.0f);
+    S.es_dot[k] = c.es_dot;
+    S.ev_dot[k] = c.ev_dot;
+    S.es[k] += c.es_dot * P.dt;
+    S.ev[k] += c.ev_dot * P.dt;
+    S.p[k] = c.p;
+    for (unsigned w = 0; w < P.nw && w < 5; ++w) S.walls_force_pp[o + (size_t)P.np * w] = c.wf[w];
+}
+
+// 6 resident blocks of 128 threads per SM (80 registers): measured best
+// between 1 and 8 on the dense-shear workload.
+#ifndef SPHB_CONTACT_MINB
+#define SPHB_CONTACT_MINB 6
+#endif
+template <int PREC, int MODEL>
+__global__ void __launch_bounds__(128, SPHB_CONTACT_MINB) k_contacts(DevParams P, DevState S)
+{
+    extern __shared__ uint32_t srow[];
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0 && S.ctl->nl_rebuild) S.ctl->nl_rebuild = 0;  // k_nl_build has run
+    if (S.ctl->err || k >= P.np) return;
+    ContactOut c;
+    if (!contact_particle<PREC, MODEL>(P, S, k, srow, blockDim.x, threadIdx.x, c)) return;
+    contact_writeback(P, S, k, c);
+}
+
+// Neighbour list of sorted particle k: every candidate closer than
+// r_a + r_b + skin, in the reference's visiting order; records the build
+// position.
+__device__ __forceinline__ void nl_build_particle(const DevParams &P, const DevState &S, unsigned k)
+{
+    double4 xa = S.x[k];
+    const double ra = xa.w;
+    unsigned n = 0;
+    const size_t np = P.np;
+    for_each_cell_candidate(P, S, k, xa, [&](unsigned b, int sx, int sy) {
+        double4 xb = S.x[b];
+        V3 dm = shift_vec(P, sx, sy);
+        V3 xab = add3(mk3(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z), dm);
+        double reach = ra + xb.w + P.skin;
+        if (dot3(xab, xab) < reach * reach) {
+            if (n < P.nlmax) S.nl[(size_t)n * np + k] = b | ((uint32_t)dm_encode(sx, sy) << 28);
+            ++n;
+        }
+        return true;
+    });
+    S.nl_count[k] = n <= P.nlmax ? n : NL_OVERFLOW;
+    S.x_ref[k] = make_float4((float)xa.x, (float)xa.y, (float)xa.z, 0.0f);
+}
+
+// Loop state an integration step reads (the values before the step).
+struct StepClock {
+    long long iter;
+    double t_current;
+    int velocity_state;
+    double tau_eff_x;
+};
+
+// integrate, src/integration.cuh:14-305 (TY3 default, TY2 selectable), for
+// sorted particle k with its force and torque, followed by the cell hash of
+// the new position (src/sorting.cuh:7-51).  Reads the current state from S
+// and writes the new x, vel, angvel (and their FP32 copies when vel_f_out
+// is set) to the *_out arrays -- S's own arrays for the in-place kernel, the
+// other buffer of a ping-pong pair for the fused step.  Raises *resort_flag
+// when the cell changed and *nl_flag when the particle left its
+// neighbour-list skin.  Returns false after raising an outside-grid error.
+__device__ __forceinline__ bool integrate_particle(const DevParams &P, const DevState &S, unsigned k,
+                                                   double4 force, double4 torque, const StepClock &clk,
+                                                   double4 *x_out, double4 *vel_out,
+                                                   double4 *angvel_out, float4 *vel_f_out,
+                                                   float4 *angvel_f_out, int *resort_flag,
+                                                   int *nl_flag)
+{
+    const long long iter = clk.iter;
+    const double t_current = clk.t_current;
+    // rate-state velocity step (device.cu:2461-2469), decided from the
+    // loop state before this step
+    int change_velocity_state = 0;
+    {
+        int vs = clk.velocity_state;
+        if (t_current >= 10.0 && t_current < 15.0 && vs == 1) change_velocity_state = 1;
+        else if (t_current >= 15.0 && vs == 2) change_velocity_state = -1;
+    }
+    const double velocity_factor = 10.0;
+    double4 angpos = S.angpos[k];
+    double4 x = S.x[k], vel = S.vel[k], angvel = S.angvel[k];
+    double4 xyzsum = S.xyzsum[k];
+    int wall0mode = 0;
+    double wall0mass = 0.0;
+    if (P.nw > 0) {
+        wall0mode = P.wmode[0];
+        wall0mass = S.wmvfd[0].x;
+    }
+    double tau_eff_x = 0.0;
+    if (P.nw > 0 && wall0mode == 3) tau_eff_x = clk.tau_eff_x;
+    double4 acc0 = make_double4(0, 0, 0, 0), angacc0 = make_double4(0, 0, 0, 0);
+    if (iter != 0) {
+        acc0 = S.acc[k];
+        angacc0 = S.angacc[k];
+    }
+    double radius = x.w;
+    double dt = P.dt;
+    double m = 4.0 / 3.0 * SPHB_PI * radius * radius * radius * P.rho;
+    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+    acc.x = force.x / m + P.g[0];
+    acc.y = force.y / m + P.g[1];
+    acc.z = force.z / m + P.g[2];
+    double4 angacc = make_double4(0.0, 0.0, 0.0, 0.0);
+    angacc.x = torque.x * 1.0 / (2.0 / 5.0 * m * radius * radius);
+    angacc.y = torque.y * 1.0 / (2.0 / 5.0 * m * radius * radius);
+    angacc.z = torque.z * 1.0 / (2.0 / 5.0 * m * radius * radius);
+    const double4 zero4 = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (wall0mode == 3 && vel.w > 0.0001 && x.z > P.L[2] * 0.5) {
+        double f_tau_x = (P.tau_x + tau_eff_x) * P.L[0] * P.L[1];
+        acc.x = f_tau_x / wall0mass;
+        acc.y = 0.0;
+        acc.z -= P.g[2];
+        angacc = zero4;
+    } else if (vel.w > 0.0001 && vel.w < 10.0) {
+        acc.x = 0.0;
+        acc.y = 0.0;
+        acc.z -= P.g[2];
+        angacc = zero4;
+    }
+    if (vel.w >= 10.0) {
+        acc.y = 0.0;
+        angacc.x = 0.0;
+        angacc.z = 0.0;
+    }
+    if (vel.w < -0.0001) {
+        acc.x = 0.0;
+        acc.y = 0.0;
+        acc.z = 0.0;
+        angacc = zero4;
+    }
+    double4 x_new, vel_new, angpos_new, angvel_new;
+    if (P.integrator == 3) {
+        double dax = (acc.x - acc0.x) / dt, day = (acc.y - acc0.y) / dt, daz = (acc.z - acc0.z) / dt;
+        double dwx = (angacc.x - angacc0.x) / dt, dwy = (angacc.y - angacc0.y) / dt,
+               dwz = (angacc.z - angacc0.z) / dt;
+        x_new.x = x.x + vel.x * dt + 0.5 * acc.x * dt * dt + 1.0 / 6.0 * dax * dt * dt * dt;
+        x_new.y = x.y + vel.y * dt + 0.5 * acc.y * dt * dt + 1.0 / 6.0 * day * dt * dt * dt;
+        x_new.z = x.z + vel.z * dt + 0.5 * acc.z * dt * dt + 1.0 / 6.0 * daz * dt * dt * dt;
+        x_new.w = x.w;
+        vel_new.x = vel.x + acc.x * dt + 0.5 * dax * dt * dt;
+        vel_new.y = vel.y + acc.y * dt + 0.5 * day * dt * dt;
+        vel_new.z = vel.z + acc.z * dt + 0.5 * daz * dt * dt;
+        vel_new.w = vel.w;
+        angpos_new.x = angpos.x + angvel.x * dt + 0.5 * angacc.x * dt * dt + 1.0 / 6.0 * dwx * dt * dt * dt;
+        angpos_new.y = angpos.y + angvel.y * dt + 0.5 * angacc.y * dt * dt + 1.0 / 6.0 * dwy * dt * dt * dt;
+        angpos_new.z = angpos.z + angvel.z * dt + 0.5 * angacc.z * dt * dt + 1.0 / 6.0 * dwz * dt * dt * dt;
+        angpos_new.w = angpos.w;
+        angvel_new.x = angvel.x + angacc.x * dt + 0.5 * dwx * dt * dt;
+        angvel_new.y = angvel.y + angacc.y * dt + 0.5 * dwy * dt * dt;
+        angvel_new.z = angvel.z + angacc.z * dt + 0.5 * dwz * dt * dt;
+        angvel_new.w = angvel.w;
+        xyzsum.x += vel.x * dt + 0.5 * acc.x * dt * dt + 1.0 / 6.0 * dax * dt * dt * dt;
+        xyzsum.y += vel.y * dt + 0.5 * acc.y * dt * dt + 1.0 / 6.0 * day * dt * dt * dt;
+        xyzsum.z += vel.z * dt + 0.5 * acc.z * dt * dt + 1.0 / 6.0 * daz * dt * dt * dt;
+    } else {
+        x_new.x = x.x + vel.x * dt + 0.5 * acc.x * dt * dt;
+        x_new.y = x.y + vel.y * dt + 0.5 * acc.y * dt * dt;
+        x_new.z = x.z + vel.z * dt + 0.5 * acc.z * dt * dt;
+        x_new.w = x.w;
+        vel_new.x = vel.x + acc.x * dt;
+        vel_new.y = vel.y + acc.y * dt;
+        vel_new.z = vel.z + acc.z * dt;
+        vel_new.w = vel.w;
+        angpos_new.x = angpos.x + angvel.x * dt + 0.5 * angacc.x * dt * dt;
+        angpos_new.y = angpos.y + angvel.y * dt + 0.5 * angacc.y * dt * dt;
+        angpos_new.z = angpos.z + angvel.z * dt + 0.5 * angacc.z * dt * dt;
+        angpos_new.w = angpos.w;
+        angvel_new.x = angvel.x + angacc.x * dt;
+        angvel_new.y = angvel.y + angacc.y * dt;
+        angvel_new.z = angvel.z + angacc.z * dt;
+        angvel_new.w = angvel.w;
+        xyzsum.x += vel.x * dt + 0.5 * acc.x * dt * dt;
+        xyzsum.y += vel.y * dt + 0.5 * acc.y * dt * dt;
+        xyzsum.z += vel.z * dt + 0.5 * acc.z * dt * dt;
+    }
+    if (P.periodic == 1) {
+        if (x_new.x < P.origo[0]) x_new.x += P.L[0];
+        if (x_new.x > P.L[0]) x_new.x -= P.L[0];
+        if (x_new.y < P.origo[1]) x_new.y += P.L[1];
+        if (x_new.y > P.L[1]) x_new.y -= P.L[1];
+    } else if (P.periodic == 2) {
+        if (x_new.x < P.origo[0]) x_new.x += P.L[0];
+        if (x_new.x > P.L[0]) x_new.x -= P.L[0];
+    }
+    if (vel.w > 5.0 && vel.w < 10.0) {
+        if (change_velocity_state == 1) vel_new.x *= velocity_factor;
+        else if (change_velocity_state == -1) vel_new.x /= velocity_factor;
+    }
+    S.xyzsum[k] = xyzsum;
+    S.acc[k] = acc;
+    S.angacc[k] = angacc;
+    angvel_out[k] = angvel_new;
+    vel_out[k] = vel_new;
+    S.angpos[k] = angpos_new;
+    x_out[k] = x_new;
+    if (vel_f_out) {
+        vel_f_out[k] = make_float4((float)vel_new.x, (float)vel_new.y, (float)vel_new.z, (float)vel_new.w);
+        angvel_f_out[k] = make_float4((float)angvel_new.x, (float)angvel_new.y, (float)angvel_new.z, 0.0f);
+    }
+    // cell of the new position
+    int ix, iy, iz;
+    if (!cell_coord(P, x_new.x, 0, ix) || !cell_coord(P, x_new.y, 1, iy) ||
+        !cell_coord(P, x_new.z, 2, iz)) {
+        raise_err(S.ctl, DERR_OUTSIDE, (int)S.orig_of[k]);
+        return false;
+    }
+    unsigned c = ((unsigned)iz * P.num[1]) * P.num[0] + (unsigned)iy * P.num[0] + (unsigned)ix;
+    S.cell_new[k] = c;
+    if (c != S.cell_of[k]) *resort_flag = 1;
+    // neighbour lists stay exact while every particle is within 0.45 skin
+    // of its position at the build
+    float4 xr = S.x_ref[k];
+    double ddx = x_new.x - (double)xr.x, ddy = x_new.y - (double)xr.y, ddz = x_new.z - (double)xr.z;
+    double lim = 0.45 * P.skin;
+    if (ddx * ddx + ddy * ddy + ddz * ddz > lim * lim) *nl_flag = 1;
+    return true;
+}
 
 }  // namespace sphb

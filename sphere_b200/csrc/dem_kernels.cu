@@ -5,31 +5,18 @@
 // src/CMakeLists.txt:25).  One thread per particle in sorted order.
 #include "dem_device.cuh"
 #include "dem_launch.h"
+#include "reduce_device.cuh"
 
 namespace sphb {
 
 // Neighbour list build: runs every step, works only when DevCtl::nl_rebuild.
+// Also refreshes the FP32 velocity copies of the mixed mode (the rebuild
+// follows every re-sort and every write of the state from the host).
 __global__ void __launch_bounds__(128) k_nl_build(DevParams P, DevState S)
 {
     unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
     if (S.ctl->err || !S.ctl->nl_rebuild || k >= P.np) return;
-    double4 xa = S.x[k];
-    const double ra = xa.w;
-    unsigned n = 0;
-    const size_t np = P.np;
-    for_each_cell_candidate(P, S, k, xa, [&](unsigned b, int sx, int sy) {
-        double4 xb = S.x[b];
-        V3 dm = shift_vec(P, sx, sy);
-        V3 xab = add3(mk3(xa.x - xb.x, xa.y - xb.y, xa.z - xb.z), dm);
-        double reach = ra + xb.w + P.skin;
-        if (dot3(xab, xab) < reach * reach) {
-            if (n < P.nlmax) S.nl[(size_t)n * np + k] = b | ((uint32_t)dm_encode(sx, sy) << 28);
-            ++n;
-        }
-        return true;
-    });
-    S.nl_count[k] = n <= P.nlmax ? n : NL_OVERFLOW;
-    S.x_ref[k] = make_float4((float)xa.x, (float)xa.y, (float)xa.z, 0.0f);
+    nl_build_particle(P, S, k);
     if (S.vel_f) {
         double4 v = S.vel[k], w = S.angvel[k];
         S.vel_f[k] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
@@ -177,23 +164,6 @@ __device__ double block_tree_sum(const double *in, unsigned np, unsigned nblocks
     return cache[0];
 }
 
-// Adds in[0..n) in index order (the reference's serial loop over block
-// partials, integration.cuh:67-68, 376-378).  All threads of the calling
-// block stage chunks in shared memory; thread 0 adds them one by one.
-__device__ double ordered_sum(const double *in, unsigned n, double *stage)
-{
-    double acc = 0.0;
-    for (unsigned base = 0; base < n; base += 2048) {
-        unsigned m = min(2048u, n - base);
-        __syncthreads();
-        for (unsigned i = threadIdx.x; i < m; i += blockDim.x) stage[i] = __ldcg(in + base + i);
-        __syncthreads();
-        if (threadIdx.x == 0)
-            for (unsigned i = 0; i < m; ++i) acc += stage[i];
-    }
-    return acc;
-}
-
 __global__ void __launch_bounds__(256) k_tau_partials(DevParams P, DevState S)
 {
     __shared__ double cache[256];
@@ -226,153 +196,13 @@ __global__ void __launch_bounds__(256) k_integrate(DevParams P, DevState S)
 {
     unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
     if (S.ctl->err || k >= P.np) return;
-    const long long iter = S.ctl->iter;
-    const double t_current = S.ctl->t_current;
-    // rate-state velocity step (device.cu:2461-2469), decided from the
-    // loop state before this step
-    int change_velocity_state = 0;
-    {
-        int vs = S.ctl->velocity_state;
-        if (t_current >= 10.0 && t_current < 15.0 && vs == 1) change_velocity_state = 1;
-        else if (t_current >= 15.0 && vs == 2) change_velocity_state = -1;
-    }
-    const double velocity_factor = 10.0;
-    double4 force = S.force[k], torque = S.torque[k], angpos = S.angpos[k];
-    double4 x = S.x[k], vel = S.vel[k], angvel = S.angvel[k];
-    double4 xyzsum = S.xyzsum[k];
-    int wall0mode = 0;
-    double wall0mass = 0.0;
-    if (P.nw > 0) {
-        wall0mode = P.wmode[0];
-        wall0mass = S.wmvfd[0].x;
-    }
-    double tau_eff_x = 0.0;
-    if (P.nw > 0 && wall0mode == 3) tau_eff_x = S.ctl->tau_eff_x;
-    double4 acc0 = make_double4(0, 0, 0, 0), angacc0 = make_double4(0, 0, 0, 0);
-    if (iter != 0) {
-        acc0 = S.acc[k];
-        angacc0 = S.angacc[k];
-    }
-    double radius = x.w;
-    double dt = P.dt;
-    double m = 4.0 / 3.0 * SPHB_PI * radius * radius * radius * P.rho;
-    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
-    acc.x = force.x / m + P.g[0];
-    acc.y = force.y / m + P.g[1];
-    acc.z = force.z / m + P.g[2];
-    double4 angacc = make_double4(0.0, 0.0, 0.0, 0.0);
-    angacc.x = torque.x * 1.0 / (2.0 / 5.0 * m * radius * radius);
-    angacc.y = torque.y * 1.0 / (2.0 / 5.0 * m * radius * radius);
-    angacc.z = torque.z * 1.0 / (2.0 / 5.0 * m * radius * radius);
-    const double4 zero4 = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (wall0mode == 3 && vel.w > 0.0001 && x.z > P.L[2] * 0.5) {
-        double f_tau_x = (P.tau_x + tau_eff_x) * P.L[0] * P.L[1];
-        acc.x = f_tau_x / wall0mass;
-        acc.y = 0.0;
-        acc.z -= P.g[2];
-        angacc = zero4;
-    } else if (vel.w > 0.0001 && vel.w < 10.0) {
-        acc.x = 0.0;
-        acc.y = 0.0;
-        acc.z -= P.g[2];
-        angacc = zero4;
-    }
-    if (vel.w >= 10.0) {
-        acc.y = 0.0;
-        angacc.x = 0.0;
-        angacc.z = 0.0;
-    }
-    if (vel.w < -0.0001) {
-        acc.x = 0.0;
-        acc.y = 0.0;
-        acc.z = 0.0;
-        angacc = zero4;
-    }
-    double4 x_new, vel_new, angpos_new, angvel_new;
-    if (P.integrator == 3) {
-        double dax = (acc.x - acc0.x) / dt, day = (acc.y - acc0.y) / dt, daz = (acc.z - acc0.z) / dt;
-        double dwx = (angacc.x - angacc0.x) / dt, dwy = (angacc.y - angacc0.y) / dt,
-               dwz = (angacc.z - angacc0.z) / dt;
-        x_new.x = x.x + vel.x * dt + 0.5 * acc.x * dt * dt + 1.0 / 6.0 * dax * dt * dt * dt;
-        x_new.y = x.y + vel.y * dt + 0.5 * acc.y * dt * dt + 1.0 / 6.0 * day * dt * dt * dt;
-        x_new.z = x.z + vel.z * dt + 0.5 * acc.z * dt * dt + 1.0 / 6.0 * daz * dt * dt * dt;
-        x_new.w = x.w;
-        vel_new.x = vel.x + acc.x * dt + 0.5 * dax * dt * dt;
-        vel_new.y = vel.y + acc.y * dt + 0.5 * day * dt * dt;
-        vel_new.z = vel.z + acc.z * dt + 0.5 * daz * dt * dt;
-        vel_new.w = vel.w;
-        angpos_new.x = angpos.x + angvel.x * dt + 0.5 * angacc.x * dt * dt + 1.0 / 6.0 * dwx * dt * dt * dt;
-        angpos_new.y = angpos.y + angvel.y * dt + 0.5 * angacc.y * dt * dt + 1.0 / 6.0 * dwy * dt * dt * dt;
-        angpos_new.z = angpos.z + angvel.z * dt + 0.5 * angacc.z * dt * dt + 1.0 / 6.0 * dwz * dt * dt * dt;
-        angpos_new.w = angpos.w;
-        angvel_new.x = angvel.x + angacc.x * dt + 0.5 * dwx * dt * dt;
-        angvel_new.y = angvel.y + angacc.y * dt + 0.5 * dwy * dt * dt;
-        angvel_new.z = angvel.z + angacc.z * dt + 0.5 * dwz * dt * dt;
-        angvel_new.w = angvel.w;
-        xyzsum.x += vel.x * dt + 0.5 * acc.x * dt * dt + 1.0 / 6.0 * dax * dt * dt * dt;
-        xyzsum.y += vel.y * dt + 0.5 * acc.y * dt * dt + 1.0 / 6.0 * day * dt * dt * dt;
-        xyzsum.z += vel.z * dt + 0.5 * acc.z * dt * dt + 1.0 / 6.0 * daz * dt * dt * dt;
-    } else {
-        x_new.x = x.x + vel.x * dt + 0.5 * acc.x * dt * dt;
-        x_new.y = x.y + vel.y * dt + 0.5 * acc.y * dt * dt;
-        x_new.z = x.z + vel.z * dt + 0.5 * acc.z * dt * dt;
-        x_new.w = x.w;
-        vel_new.x = vel.x + acc.x * dt;
-        vel_new.y = vel.y + acc.y * dt;
-        vel_new.z = vel.z + acc.z * dt;
-        vel_new.w = vel.w;
-        angpos_new.x = angpos.x + angvel.x * dt + 0.5 * angacc.x * dt * dt;
-        angpos_new.y = angpos.y + angvel.y * dt + 0.5 * angacc.y * dt * dt;
-        angpos_new.z = angpos.z + angvel.z * dt + 0.5 * angacc.z * dt * dt;
-        angpos_new.w = angpos.w;
-        angvel_new.x = angvel.x + angacc.x * dt;
-        angvel_new.y = angvel.y + angacc.y * dt;
-        angvel_new.z = angvel.z + angacc.z * dt;
-        angvel_new.w = angvel.w;
-        xyzsum.x += vel.x * dt + 0.5 * acc.x * dt * dt;
-        xyzsum.y += vel.y * dt + 0.5 * acc.y * dt * dt;
-        xyzsum.z += vel.z * dt + 0.5 * acc.z * dt * dt;
-    }
-    if (P.periodic == 1) {
-        if (x_new.x < P.origo[0]) x_new.x += P.L[0];
-        if (x_new.x > P.L[0]) x_new.x -= P.L[0];
-        if (x_new.y < P.origo[1]) x_new.y += P.L[1];
-        if (x_new.y > P.L[1]) x_new.y -= P.L[1];
-    } else if (P.periodic == 2) {
-        if (x_new.x < P.origo[0]) x_new.x += P.L[0];
-        if (x_new.x > P.L[0]) x_new.x -= P.L[0];
-    }
-    if (vel.w > 5.0 && vel.w < 10.0) {
-        if (change_velocity_state == 1) vel_new.x *= velocity_factor;
-        else if (change_velocity_state == -1) vel_new.x /= velocity_factor;
-    }
-    S.xyzsum[k] = xyzsum;
-    S.acc[k] = acc;
-    S.angacc[k] = angacc;
-    S.angvel[k] = angvel_new;
-    S.vel[k] = vel_new;
-    S.angpos[k] = angpos_new;
-    S.x[k] = x_new;
-    if (S.vel_f) {
-        S.vel_f[k] = make_float4((float)vel_new.x, (float)vel_new.y, (float)vel_new.z, (float)vel_new.w);
-        S.angvel_f[k] = make_float4((float)angvel_new.x, (float)angvel_new.y, (float)angvel_new.z, 0.0f);
-    }
-    // cell of the new position
-    int ix, iy, iz;
-    if (!cell_coord(P, x_new.x, 0, ix) || !cell_coord(P, x_new.y, 1, iy) ||
-        !cell_coord(P, x_new.z, 2, iz)) {
-        raise_err(S.ctl, DERR_OUTSIDE, (int)S.orig_of[k]);
-        return;
-    }
-    unsigned c = ((unsigned)iz * P.num[1]) * P.num[0] + (unsigned)iy * P.num[0] + (unsigned)ix;
-    S.cell_new[k] = c;
-    if (c != S.cell_of[k]) S.ctl->resort = 1;
-    // neighbour lists stay exact while every particle is within 0.45 skin
-    // of its position at the build
-    float4 xr = S.x_ref[k];
-    double ddx = x_new.x - (double)xr.x, ddy = x_new.y - (double)xr.y, ddz = x_new.z - (double)xr.z;
-    double lim = 0.45 * P.skin;
-    if (ddx * ddx + ddy * ddy + ddz * ddz > lim * lim) S.ctl->nl_rebuild = 1;
+    StepClock clk;
+    clk.iter = S.ctl->iter;
+    clk.t_current = S.ctl->t_current;
+    clk.velocity_state = S.ctl->velocity_state;
+    clk.tau_eff_x = S.ctl->tau_eff_x;
+    integrate_particle(P, S, k, S.force[k], S.torque[k], clk, S.x, S.vel, S.angvel, S.vel_f,
+                       S.angvel_f, &S.ctl->resort, &S.ctl->nl_rebuild);
 }
 
 // Cell hash of the current positions (first step, after sph_set).
@@ -419,35 +249,9 @@ __global__ void __launch_bounds__(256) k_walls_and_clock(DevParams P, DevState S
     if (threadIdx.x != 0) return;
     const long long iter = ctl->iter;
     const double t_current = ctl->t_current;
-    const double dt = P.dt;
-    for (unsigned w = 0; w < P.nw; ++w) {
-        double4 w_nx = S.wnx[w], w_mvfd = S.wmvfd[w];
-        int wmode = P.wmode[w];
-        if (wmode == 0) continue;
-        double acc0 = iter == 0 ? 0.0 : S.wacc[w];
-        w_mvfd.z = 0.0;
-        w_mvfd.z += wforce;
-        double sigma_0 = w_mvfd.w + P.sigma0_A * sin(2.0 * SPHB_PI * P.sigma0_f * t_current);
-        double N = -sigma_0 * P.L[0] * P.L[1];
-        double acc = (w_mvfd.z + N) / w_mvfd.x;
-        if (wmode == 2) acc = 0.0;
-        if (P.integrator == 3) {
-            double dacc_dt = (acc - acc0) / dt;
-            w_nx.w += w_mvfd.y * dt + 0.5 * acc * dt * dt + 1.0 / 6.0 * dacc_dt * dt * dt * dt;
-            w_mvfd.y += acc * dt + 0.5 * dacc_dt * dt * dt;
-        } else {
-            w_nx.w += w_mvfd.y * dt + 0.5 * acc * dt * dt;
-            w_mvfd.y += acc * dt;
-        }
-        S.wnx[w] = w_nx;
-        S.wmvfd[w] = w_mvfd;
-        S.wacc[w] = acc;
-    }
-    // rate-state bookkeeping (device.cu:2461-2469)
-    int vs = ctl->velocity_state;
-    if (t_current >= 10.0 && t_current < 15.0 && vs == 1) ctl->velocity_state = 2;
-    else if (t_current >= 15.0 && vs == 2) ctl->velocity_state = 1;
-    ctl->t_current = t_current + dt;
+    walls_integrate(P, S, wforce, iter, t_current);
+    ctl->velocity_state = next_velocity_state(ctl->velocity_state, t_current);
+    ctl->t_current = t_current + P.dt;
     ctl->iter = iter + 1;
     ctl->ticket = 0;
 }

@@ -33,6 +33,11 @@ struct DevState {
     // in sorted order and FP32 tangential history per slot
     float4 *vel_f, *angvel_f, *delta_t_f;
 
+    // the other buffer of the ping-pong pairs the fused step integrates into
+    // (the per-stage kernels integrate in place and never touch them)
+    double4 *x_nx, *vel_nx, *angvel_nx;
+    float4 *vel_f_nx, *angvel_f_nx;
+
     // neighbour lists in sorted order: entry j of particle k at nl[j*np + k]
     // = sorted index | periodic shift code << 28
     uint32_t *nl, *nl_count;

@@ -66,6 +66,15 @@ struct V3 {
     double x, y, z;
 };
 
+// L2-only (L1-bypassing) load of a double4, for data another block wrote
+// earlier in the same kernel.
+__device__ __forceinline__ double4 ldcg4(const double4 *p)
+{
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    double2 a = __ldcg(q), b = __ldcg(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
 __device__ __forceinline__ V3 mk3(double x, double y, double z) { return V3{x, y, z}; }
 __device__ __forceinline__ V3 add3(V3 a, V3 b) { return mk3(a.x + b.x, a.y + b.y, a.z + b.z); }
 __device__ __forceinline__ V3 sub3(V3 a, V3 b) { return mk3(a.x - b.x, a.y - b.y, a.z - b.z); }

@@ -65,6 +65,7 @@ Engine::~Engine()
 {
     conv_close();
     darcy_free();
+    persist_free();
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (void *p : allocations) cudaFree(p);
     if (host_pinned) cudaFreeHost(host_pinned);
@@ -139,6 +140,14 @@ int Engine::allocate_and_upload()
         S.vel_f = dalloc<float4>(n);
         S.angvel_f = dalloc<float4>(n);
         S.delta_t_f = dalloc<float4>(slots);
+    }
+    if (persist_eligible()) {
+        S.x_nx = dalloc<double4>(n); S.vel_nx = dalloc<double4>(n); S.angvel_nx = dalloc<double4>(n);
+        if (precision == SPH_PREC_MIXED) {
+            S.vel_f_nx = dalloc<float4>(n);
+            S.angvel_f_nx = dalloc<float4>(n);
+        }
+        if (!S.x_nx || !S.vel_nx || !S.angvel_nx) return fail(ST_CUDA, "device allocation failed");
     }
     S.nl = dalloc<uint32_t>(n * (size_t)nlmax);
     S.nl_count = dalloc<uint32_t>(n);
@@ -363,6 +372,7 @@ int Engine::ensure_graph()
 int Engine::step(uint64_t n)
 {
     if (n == 0) return ST_OK;
+    if (persist) return step_persistent(n);
     if (!warmed) {
         // one eager step first: sets kernel attributes outside any capture
         cudaError_t e = enqueue_step();
@@ -576,6 +586,7 @@ int Engine::set(int f, const void *src, size_t bytes)
         static const int one = 1;
         e = cudaMemcpyAsync(&S.ctl->nl_rebuild, &one, sizeof one, cudaMemcpyHostToDevice, stream);
     }
+    if (e == cudaSuccess) e = launch_refresh_f(P, S, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cuda_fail(e, "set");
     return poll_errors("set");
@@ -735,6 +746,7 @@ static int open_common(std::unique_ptr<Engine> &eng, const sph_opts *opts)
     e.verbose = o.verbose;
     e.graph_steps = o.graph_steps > 0 ? o.graph_steps : 64;
     e.warm_start = o.warm_start;
+    e.step_kernel = o.step_kernel;
     e.outdir = o.output_dir ? o.output_dir : "output";
     if (e.precision != SPH_PREC_FAITHFUL && e.precision != SPH_PREC_FP64 &&
         e.precision != SPH_PREC_MIXED)
@@ -756,9 +768,15 @@ static int open_common(std::unique_ptr<Engine> &eng, const sph_opts *opts)
         rc = e.mixed_init();
         if (rc) return rc;
     }
+    if (e.step_kernel == 2 && !e.persist_eligible())
+        return e.fail(sphb::ST_UNSUPPORTED, "the fused step kernel does not cover bonds, fluid or "
+                                            "the shear-stress wall (wmode 3)");
     rc = e.allocate_and_upload();
     if (rc) return rc;
-    return e.darcy_init();
+    rc = e.darcy_init();
+    if (rc) return rc;
+    e.make_views();
+    return e.persist_init();
 }
 
 static std::string sid_from_path(const char *path)
@@ -811,6 +829,35 @@ int sph_open_buffer(const void *bytes, size_t nbytes, const sph_opts *opts, cons
 }
 
 const char *sph_open_error(void) { return sphb::g_open_error.c_str(); }
+
+}  // extern "C"
+
+namespace sphb {
+
+// Opens one engine from a file path or from the bytes of a .bin file (the
+// batch engine opens its boxes with this).
+int open_engine(const char *path, const void *bytes, size_t nbytes, const sph_opts *opts,
+                const char *sid, std::unique_ptr<Engine> &out, std::string &err)
+{
+    auto eng = std::make_unique<Engine>();
+    int fluid = opts ? opts->fluid : 0;
+    int rc = path ? read_bin_file(path, fluid, eng->hs, eng->err)
+                  : parse_bin((const uint8_t *)bytes, nbytes, fluid, eng->hs, eng->err);
+    if (rc == 0) {
+        eng->sid = path ? sid_from_path(path) : (sid ? sid : "unnamed");
+        rc = open_common(eng, opts);
+    }
+    if (rc < 0) {
+        err = eng->err;
+        return rc;
+    }
+    out = std::move(eng);
+    return rc;
+}
+
+}  // namespace sphb
+
+extern "C" {
 
 int sph_check_file(const char *bin_path, int fluid)
 {

@@ -3,6 +3,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -16,6 +17,10 @@ namespace sphb {
 
 struct DarcyDev;   // Darcy solver state (darcy.cu)
 struct MixedDev;   // mixed-precision state (dem_mixed.cu)
+struct PersistDev; // fused persistent step path (engine_persist.cu)
+
+// FP32 velocity copies of the mixed mode from the FP64 velocities.
+cudaError_t launch_refresh_f(const DevParams &P, const DevState &S, cudaStream_t st);
 
 class Engine {
 public:
@@ -29,6 +34,7 @@ public:
     int verbose = 0;
     int graph_steps = 64;
     int warm_start = 0;
+    int step_kernel = 0;          // 0 automatic, 1 per-stage kernels, 2 persistent
     std::string outdir = "output";
     std::string sid = "unnamed";
 
@@ -55,6 +61,9 @@ public:
 
     DarcyDev *darcy = nullptr;
     MixedDev *mixed = nullptr;
+    PersistDev *persist = nullptr;
+    DevState S_view[2]{};         // S_view[v]: buffer view v (S is the current one)
+    int cur_view = 0;
     FILE *convlog = nullptr;
     int jacobi_grid = 0;            // blocks of the cooperative Jacobi launch
     int darcy_exact_stop = 0;       // 1: stop at the first converged iteration
@@ -101,7 +110,22 @@ public:
 
     // mixed precision
     int mixed_init();
+
+    // fused persistent step path
+    bool persist_eligible() const;
+    void make_views();
+    int persist_init();
+    void persist_free();
+    unsigned persist_grid(int shape) const;
+    cudaError_t persist_launch(uint64_t n, int shape, unsigned grid);
+    int step_persistent(uint64_t n);
+    int persist_after(uint64_t n);
+    void *persist_ctl() const;    // the box's PersistCtl on the device
 };
+
+// Opens one engine from a .bin path (path != null) or from its bytes.
+int open_engine(const char *path, const void *bytes, size_t nbytes, const struct sph_opts *opts,
+                const char *sid, std::unique_ptr<Engine> &out, std::string &err);
 
 // Zero-filled device array owned by the engine (released in ~Engine).
 template <class T> T *Engine::dalloc(size_t n)

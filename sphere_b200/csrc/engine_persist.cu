@@ -1,0 +1,214 @@
+// The engine's fused persistent step path (persistent.cuh) for one box:
+// state views for the ping-pong buffers, the launch, and an autotuner that
+// picks the block shape and grid from timed trial launches made of real
+// steps (every shape computes the same results, so trials change nothing
+// but the clock).
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "engine_internal.h"
+#include "persistent_launch.h"
+#include "dem_launch.h"
+
+namespace sphb {
+
+struct PersistDev {
+    PersistCtl *pc = nullptr;
+    BoxRec *table = nullptr;
+    unsigned *order = nullptr;
+    unsigned char *sync = nullptr;    // next counter, abort flag, group barriers
+    size_t sync_bytes = 0;
+    int shape = 1;
+    unsigned grid = 0;
+    bool tuned = false;
+    int sms = 0;
+};
+
+namespace {
+
+// layout of the sync block: [next u32][abort i32][any_err i32][pad][GroupSync ...]
+constexpr size_t kSyncHeader = 16;
+
+__global__ void k_refresh_f(DevParams P, DevState S)
+{
+    unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.np || !S.vel_f) return;
+    double4 v = S.vel[k], w = S.angvel[k];
+    S.vel_f[k] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
+    S.angvel_f[k] = make_float4((float)w.x, (float)w.y, (float)w.z, 0.0f);
+}
+
+}  // namespace
+
+cudaError_t launch_refresh_f(const DevParams &P, const DevState &S, cudaStream_t st)
+{
+    if (P.np == 0 || !S.vel_f) return cudaSuccess;
+    k_refresh_f<<<(P.np + 255) / 256, 256, 0, st>>>(P, S);
+    return cudaGetLastError();
+}
+
+bool Engine::persist_eligible() const
+{
+    if (step_kernel == 1) return false;
+    // the fused step covers dry runs without bonds or the shear-stress wall
+    return !hs.fluid && hs.nb0 == 0 && !(hs.nw > 0 && hs.wmode[0] == 3) && hs.np > 0;
+}
+
+void Engine::make_views()
+{
+    S_view[0] = S;
+    S_view[1] = S;
+    std::swap(S_view[1].x, S_view[1].x_nx);
+    std::swap(S_view[1].vel, S_view[1].vel_nx);
+    std::swap(S_view[1].angvel, S_view[1].angvel_nx);
+    std::swap(S_view[1].vel_f, S_view[1].vel_f_nx);
+    std::swap(S_view[1].angvel_f, S_view[1].angvel_f_nx);
+}
+
+int Engine::persist_init()
+{
+    if (!persist_eligible()) return ST_OK;
+    persist = new PersistDev();
+    PersistDev &D = *persist;
+    D.pc = dalloc<PersistCtl>(1);
+    D.table = dalloc<BoxRec>(1);
+    D.order = dalloc<unsigned>(1);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&D.sms, cudaDevAttrMultiProcessorCount, dev);
+    // at most one group per block of the largest grid
+    D.sync_bytes = kSyncHeader + sizeof(GroupSync) * (size_t)D.sms * 32;
+    D.sync = dalloc<unsigned char>(D.sync_bytes);
+    if (!D.pc || !D.table || !D.order || !D.sync) return fail(ST_CUDA, "device allocation failed");
+    BoxRec r;
+    std::memset(&r, 0, sizeof r);
+    r.P = P;
+    r.S[0] = S_view[0];
+    r.S[1] = S_view[1];
+    r.pc = D.pc;
+    r.scratch = S.perm_scratch;
+    r.nblk = P.nblocks256;
+    unsigned zero = 0;
+    cudaMemcpyAsync(D.table, &r, sizeof r, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(D.order, &zero, 4, cudaMemcpyHostToDevice, stream);
+    cudaError_t e = launch_refresh_f(P, S, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "persistent setup");
+    D.shape = 1;
+    D.grid = persist_grid(D.shape);
+    if (D.grid == 0) return fail(ST_CUDA, "persistent step kernel cannot be resident");
+    return ST_OK;
+}
+
+void *Engine::persist_ctl() const { return persist ? (void *)persist->pc : nullptr; }
+
+void Engine::persist_free()
+{
+    delete persist;
+    persist = nullptr;
+}
+
+unsigned Engine::persist_grid(int shape) const
+{
+    const int prec = precision;
+    const int threads = kPersistShapes[shape].threads;
+    size_t smem = persistent_smem(threads, capacity);
+    int per_sm = persistent_blocks_per_sm(prec, (int)hs.contactmodel, shape, smem);
+    if (per_sm <= 0) return 0;
+    unsigned grid = (unsigned)(per_sm * persist->sms);
+    unsigned need = (unsigned)((hs.np + threads - 1) / threads);
+    return std::max(1u, std::min(grid, need));
+}
+
+cudaError_t Engine::persist_launch(uint64_t n, int shape, unsigned grid)
+{
+    PersistDev &D = *persist;
+    const int threads = kPersistShapes[shape].threads;
+    cudaError_t e = cudaMemsetAsync(D.sync, 0, D.sync_bytes, stream);
+    if (e != cudaSuccess) return e;
+    BatchArgs A;
+    A.boxes = D.table;
+    A.nbox = 1;
+    A.order = D.order;
+    A.next = reinterpret_cast<unsigned *>(D.sync);
+    A.abort = reinterpret_cast<int *>(D.sync + 4);
+    A.any_err = reinterpret_cast<int *>(D.sync + 8);
+    A.groups = reinterpret_cast<GroupSync *>(D.sync + kSyncHeader);
+    A.group_size = grid;
+    A.nsteps = (unsigned)n;
+    return persistent_launch(precision, (int)hs.contactmodel, shape, A, grid,
+                             persistent_smem(threads, capacity), stream);
+}
+
+// Runs n steps on the persistent path.  The first call with enough steps
+// times each block shape on real steps and keeps the fastest.
+int Engine::step_persistent(uint64_t n)
+{
+    PersistDev &D = *persist;
+    uint64_t done = 0;
+    const uint64_t trial = 8;
+    if (!D.tuned && n >= trial * (kNumPersistShapes + 1)) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        float best = 1e30f;
+        int best_shape = D.shape;
+        for (int sh = 0; sh < kNumPersistShapes; ++sh) {
+            unsigned g = persist_grid(sh);
+            if (!g) continue;
+            cudaEventRecord(a, stream);
+            cudaError_t e = persist_launch(trial, sh, g);
+            cudaEventRecord(b, stream);
+            if (e != cudaSuccess) {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+                return cuda_fail(e, "persistent step");
+            }
+            cudaEventSynchronize(b);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            done += trial;
+            int rc = persist_after(trial);
+            if (rc) {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+                return rc;
+            }
+            if (ms < best) {
+                best = ms;
+                best_shape = sh;
+            }
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        D.shape = best_shape;
+        D.grid = persist_grid(best_shape);
+        D.tuned = true;
+    }
+    if (done < n) {
+        cudaError_t e = persist_launch(n - done, D.shape, D.grid);
+        if (e != cudaSuccess) return cuda_fail(e, "persistent step");
+        return persist_after(n - done);
+    }
+    return ST_OK;
+}
+
+// After a launch of n steps: advance the host mirrors, pick up the current
+// view and report device errors.
+int Engine::persist_after(uint64_t n)
+{
+    PersistDev &D = *persist;
+    int view = 0, abort = 0;
+    cudaMemcpyAsync(&view, &D.pc->view, 4, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(&abort, D.sync + 4, 4, cudaMemcpyDeviceToHost, stream);
+    advance_host_clock(n);
+    int rc = poll_errors("step");
+    cur_view = view & 1;
+    S = S_view[cur_view];
+    if (rc) return rc;
+    if (abort) return fail(ST_TIMEOUT, "step: a bounded device wait timed out");
+    return ST_OK;
+}
+
+}  // namespace sphb

@@ -44,7 +44,8 @@ class SphOpts(ctypes.Structure):
     _fields_ = [("fluid", ctypes.c_int), ("device", ctypes.c_int), ("verbose", ctypes.c_int),
                 ("precision", ctypes.c_int), ("integrator", ctypes.c_int),
                 ("contact_capacity", ctypes.c_int), ("warm_start", ctypes.c_int),
-                ("graph_steps", ctypes.c_int), ("output_dir", ctypes.c_char_p)]
+                ("graph_steps", ctypes.c_int), ("output_dir", ctypes.c_char_p),
+                ("step_kernel", ctypes.c_int)]
 
 
 class SphInfo(ctypes.Structure):
@@ -63,6 +64,16 @@ class SphProfile(ctypes.Structure):
                 ("bonds_ms", ctypes.c_double), ("fluid_ms", ctypes.c_double),
                 ("integrate_ms", ctypes.c_double), ("step_ms", ctypes.c_double),
                 ("steps", ctypes.c_uint64)]
+
+
+class SphBatchConfig(ctypes.Structure):
+    _fields_ = [("threads", ctypes.c_int), ("group_size", ctypes.c_int), ("grid", ctypes.c_int),
+                ("tuned", ctypes.c_int), ("ntrials", ctypes.c_int), ("graph", ctypes.c_int)]
+
+
+class SphBatchTrial(ctypes.Structure):
+    _fields_ = [("threads", ctypes.c_int), ("group_size", ctypes.c_int), ("grid", ctypes.c_int),
+                ("ms_per_step", ctypes.c_double)]
 
 
 class EngineError(RuntimeError):
@@ -104,12 +115,36 @@ def lib() -> ctypes.CDLL:
     L.sph_check_file.restype = ctypes.c_int
     L.sph_close.argtypes = [P]
     L.sph_version.restype = ctypes.c_char_p
+    # batches
+    L.sph_open_batch_buffers.argtypes = [ctypes.POINTER(ctypes.c_void_p),
+                                         ctypes.POINTER(ctypes.c_size_t), ctypes.c_int,
+                                         ctypes.POINTER(SphOpts), ctypes.POINTER(P)]
+    L.sph_open_batch.argtypes = [ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
+                                 ctypes.POINTER(SphOpts), ctypes.POINTER(P)]
+    L.sph_batch_open_error.restype = ctypes.c_char_p
+    L.sph_batch_step.argtypes = [P, ctypes.c_uint64]
+    L.sph_batch_step_timed.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
+    L.sph_batch_autotune.argtypes = [P, ctypes.c_uint64]
+    L.sph_batch_size.argtypes = [P]
+    L.sph_batch_field_bytes.argtypes = [P, ctypes.c_int, ctypes.c_int]
+    L.sph_batch_field_bytes.restype = ctypes.c_int64
+    L.sph_batch_get.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]
+    L.sph_batch_write_bin.argtypes = [P, ctypes.c_int, ctypes.c_char_p]
+    L.sph_batch_get_config.argtypes = [P, ctypes.POINTER(SphBatchConfig)]
+    L.sph_batch_get_trials.argtypes = [P, ctypes.POINTER(SphBatchTrial), ctypes.c_int]
+    L.sph_batch_last_error.argtypes = [P]
+    L.sph_batch_last_error.restype = ctypes.c_char_p
+    L.sph_batch_close.argtypes = [P]
     _lib = L
     return L
 
 
+STEP_KERNEL = {"auto": 0, "stages": 1, "persistent": 2}
+
+
 def make_opts(fluid=False, precision="faithful", integrator=3, capacity=32, device=-1,
-              graph_steps=0, warm_start=False, verbose=False, output_dir=None) -> SphOpts:
+              graph_steps=0, warm_start=False, verbose=False, output_dir=None,
+              step_kernel="auto") -> SphOpts:
     o = SphOpts()
     lib().sph_default_opts(ctypes.byref(o))
     o.fluid = int(bool(fluid))
@@ -121,6 +156,7 @@ def make_opts(fluid=False, precision="faithful", integrator=3, capacity=32, devi
     o.warm_start = int(bool(warm_start))
     o.verbose = int(bool(verbose))
     o.output_dir = os.fsencode(output_dir) if output_dir else None
+    o.step_kernel = STEP_KERNEL[step_kernel] if isinstance(step_kernel, str) else int(step_kernel)
     return o
 
 
@@ -134,19 +170,19 @@ class Engine:
 
     def __init__(self, source: Union[str, os.PathLike, binfile.BinData], fluid: Optional[bool] = None,
                  precision="faithful", integrator=3, capacity=32, device=-1, graph_steps=0,
-                 warm_start=False, verbose=False, output_dir=None, sid=None):
+                 warm_start=False, verbose=False, output_dir=None, sid=None, step_kernel="auto"):
         L = lib()
         h = ctypes.c_void_p()
         if isinstance(source, binfile.BinData):
             fl = source.fluid if fluid is None else fluid
             self._opts = make_opts(fl, precision, integrator, capacity, device, graph_steps,
-                                   warm_start, verbose, output_dir)
+                                   warm_start, verbose, output_dir, step_kernel)
             buf = binfile.serialize_bin(source)
             rc = L.sph_open_buffer(buf, len(buf), ctypes.byref(self._opts),
                                    (sid or "unnamed").encode(), ctypes.byref(h))
         else:
             self._opts = make_opts(bool(fluid), precision, integrator, capacity, device,
-                                   graph_steps, warm_start, verbose, output_dir)
+                                   graph_steps, warm_start, verbose, output_dir, step_kernel)
             rc = L.sph_open(os.fsencode(source), ctypes.byref(self._opts), ctypes.byref(h))
         if rc < 0 or not h.value:
             raise EngineError(rc, L.sph_open_error().decode())
@@ -233,3 +269,93 @@ def check_file(path, fluid=False):
     L = lib()
     rc = L.sph_check_file(os.fsencode(path), int(bool(fluid)))
     return rc, (L.sph_open_error().decode() if rc else "")
+
+
+def _shape_of(name, nbytes):
+    if name in _VEC4:
+        return numpy.float64, (nbytes // 32, 4)
+    if name in _U32:
+        return numpy.uint32, (nbytes // 4,)
+    if name in _I64:
+        return numpy.int64, (nbytes // 8,)
+    if name == "darcy_v":
+        return numpy.float64, (nbytes // 24, 3)
+    return numpy.float64, (nbytes // 8,)
+
+
+class Batch:
+    """Many independent dry boxes stepped by one launch of the fused
+    persistent step kernel (``sph_open_batch``).  ``boxes`` are
+    :class:`~sphere_b200.binfile.BinData` objects or .bin paths."""
+
+    def __init__(self, boxes, precision="mixed", integrator=3, capacity=32, device=-1):
+        L = lib()
+        self._opts = make_opts(False, precision, integrator, capacity, device)
+        bufs = [binfile.serialize_bin(b) if isinstance(b, binfile.BinData)
+                else open(b, "rb").read() for b in boxes]
+        n = len(bufs)
+        self._keep = [ctypes.create_string_buffer(b, len(b)) for b in bufs]
+        ptrs = (ctypes.c_void_p * n)(*[ctypes.cast(k, ctypes.c_void_p) for k in self._keep])
+        sizes = (ctypes.c_size_t * n)(*[len(b) for b in bufs])
+        h = ctypes.c_void_p()
+        rc = L.sph_open_batch_buffers(ptrs, sizes, n, ctypes.byref(self._opts), ctypes.byref(h))
+        self._keep = None
+        if rc < 0 or not h.value:
+            raise EngineError(rc, L.sph_batch_open_error().decode())
+        self._h = h
+        self.nbox = n
+
+    def _check(self, rc):
+        if rc < 0:
+            raise EngineError(rc, lib().sph_batch_last_error(self._h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().sph_batch_close(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def step(self, n=1) -> int:
+        return self._check(lib().sph_batch_step(self._h, int(n)))
+
+    def step_timed(self, n) -> float:
+        ms = ctypes.c_double(0.0)
+        self._check(lib().sph_batch_step_timed(self._h, int(n), ctypes.byref(ms)))
+        return ms.value
+
+    def autotune(self, trial_steps=4) -> int:
+        return self._check(lib().sph_batch_autotune(self._h, int(trial_steps)))
+
+    def config(self) -> dict:
+        c = SphBatchConfig()
+        self._check(lib().sph_batch_get_config(self._h, ctypes.byref(c)))
+        return {f: getattr(c, f) for f, _ in c._fields_}
+
+    def trials(self) -> list:
+        n = self._check(lib().sph_batch_get_trials(self._h, None, 0))
+        arr = (SphBatchTrial * max(n, 1))()
+        self._check(lib().sph_batch_get_trials(self._h, arr, n))
+        return [{f: getattr(arr[i], f) for f, _ in SphBatchTrial._fields_} for i in range(n)]
+
+    def get(self, box, name) -> numpy.ndarray:
+        nbytes = int(lib().sph_batch_field_bytes(self._h, int(box), FIELD_ID[name]))
+        dtype, shape = _shape_of(name, nbytes)
+        out = numpy.empty(shape, dtype=dtype)
+        self._check(lib().sph_batch_get(self._h, int(box), FIELD_ID[name], out.ctypes.data,
+                                        out.nbytes))
+        return out
+
+    def write_bin(self, box, path) -> None:
+        self._check(lib().sph_batch_write_bin(self._h, int(box), os.fsencode(path)))

@@ -60,12 +60,15 @@ def cases():
 
 @pytest.mark.parametrize("name,data", list(cases()), ids=[c[0] for c in cases()])
 @pytest.mark.parametrize("precision", ["faithful", "fp64"])
-def test_step_parity(tmp_path, name, data, precision):
+@pytest.mark.parametrize("kernel", ["stages", "persistent"])
+def test_step_parity(tmp_path, name, data, precision, kernel):
+    """Both step paths -- the per-stage kernels and the fused persistent
+    kernel -- against the oracle, bit for bit."""
     from sphere_b200.engine import Engine
     path = tmp_path / f"{name}.bin"
     binfile.write_bin(data, path)
     orc = O.Oracle(str(path), precision="faithful" if precision == "faithful" else "fp64")
-    eng = Engine(str(path), precision=precision, graph_steps=8)
+    eng = Engine(str(path), precision=precision, graph_steps=8, step_kernel=kernel)
     for k, n in enumerate((1, 1, 3, 10, 25)):
         assert eng.step(n) == 0
         assert orc.step(n) == 0, orc.error()
@@ -74,3 +77,38 @@ def test_step_parity(tmp_path, name, data, precision):
     occupied = (orc.get("contacts") != data.np).sum()
     assert occupied > 0 or data.contactmodel == 1
     eng.close()
+
+
+@pytest.mark.parametrize("precision", ["faithful", "fp64"])
+def test_persistent_autotuned_run(tmp_path, precision):
+    """A call long enough to start the block-shape autotuner (trial launches
+    of every shape on real steps) still advances exactly like the oracle."""
+    from sphere_b200.engine import Engine
+    d = dense(6, n=700)
+    configs.shear_setup(d, 0.05, 20e3)
+    d.w_x[0] -= 0.003
+    path = tmp_path / "tuned.bin"
+    binfile.write_bin(d, path)
+    orc = O.Oracle(str(path), precision=precision)
+    eng = Engine(str(path), precision=precision, step_kernel="persistent")
+    for n in (60, 7):
+        assert eng.step(n) == 0
+        assert orc.step(n) == 0, orc.error()
+        bad = compare(eng, orc)
+        assert not bad, bad
+    assert int(eng.get("iter")[0]) == 67
+    eng.close()
+
+
+def test_persistent_refuses_bonds(tmp_path):
+    """The fused step does not cover bonds: asking for it is an error, the
+    automatic choice falls back to the per-stage kernels."""
+    from sphere_b200.engine import Engine, EngineError
+    from helpers import bonded_packing
+    d = bonded_packing(configs, n=300, seed=3)
+    path = tmp_path / "bonded.bin"
+    binfile.write_bin(d, path)
+    with pytest.raises(EngineError):
+        Engine(str(path), step_kernel="persistent")
+    with Engine(str(path)) as eng:
+        assert eng.step(2) == 0
