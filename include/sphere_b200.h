@@ -101,6 +101,9 @@ typedef enum sph_field {
     SPH_F_DARCY_ITERS_TOTAL, /* 1 int64: Jacobi iterations since open */
     SPH_F_DARCY_ITERS_EXACT, /* 1 int64: first iteration of the last solve whose
                                 residual met the tolerance (-1: none) */
+    SPH_F_DARCY_WARM,   /* 4 x 8 bytes: warm-start predictions, training steps,
+                           solves started from the network's guess (int64),
+                           last training loss (double) */
     SPH_F_BONDS,        /* nb0 x 2 u32 */
     SPH_F_BONDS_DELTA,  /* nb0 x 4 doubles (t.x, t.y, t.z, n) */
     SPH_F_BONDS_OMEGA,
@@ -259,6 +262,25 @@ int sph_batch_get_config(sph_batch *b, sph_batch_config *cfg);
 int sph_batch_get_trials(sph_batch *b, sph_batch_trial *out, int max);
 const char *sph_batch_last_error(sph_batch *b);
 void sph_batch_close(sph_batch *b);
+
+/* ---------------------------------------------------------------------
+ * The warm-start network alone (3 -> 16 -> 16 -> 1 channels, 3x3x3
+ * kernels, ReLU; BF16 tensor-core kernels with FP32 accumulation) on host
+ * arrays, for gradient checks.  The engine uses it through
+ * sph_opts.warm_start.  Layer parameters: w [27 taps][16 out][16 in]
+ * (taps z-major, then y, then x, offsets -1..1), b [16].  Inputs: 3
+ * normalised channels per cell (x fastest); output: channel 0 of layer 3.
+ * --------------------------------------------------------------------- */
+typedef struct sph_wsnet sph_wsnet;
+int sph_wsnet_create(int nx, int ny, int nz, uint64_t seed, sph_wsnet **out);
+int sph_wsnet_set_params(sph_wsnet *n, int layer, const float *w, const float *b);
+int sph_wsnet_get_params(sph_wsnet *n, int layer, float *w, float *b);
+int sph_wsnet_forward(sph_wsnet *n, const float *x3, float *out);
+/* Gradients of the mean squared error over free cells (free_cells[c] != 0)
+ * between the output and target: dw = 3 x [27][16][16], db = 3 x [16]. */
+int sph_wsnet_gradients(sph_wsnet *n, const float *x3, const float *target,
+                        const unsigned char *free_cells, float *dw, float *db);
+void sph_wsnet_destroy(sph_wsnet *n);
 
 #ifdef __cplusplus
 }

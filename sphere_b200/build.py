@@ -23,7 +23,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
 NO_FMA = {"dem_kernels.cu", "sort.cu", "darcy.cu", "persistent_fp64.cu"}
 SOURCES = ["bin_io.cpp", "dem_kernels.cu", "sort.cu", "engine.cu", "darcy.cu", "dem_mixed.cu",
            "noalloc_sort.cu", "engine_persist.cu", "persistent_fp64.cu", "persistent_mixed.cu",
-           "batch.cu"]
+           "batch.cu", "warmstart.cu"]
 
 
 def nvcc() -> str:

@@ -24,10 +24,6 @@
 
 namespace sphb {
 
-namespace {
-constexpr size_t kSyncHeader = 16;   // next, abort, any_err, pad
-}
-
 struct BatchEngine {
     std::vector<std::unique_ptr<Engine>> boxes;
     cudaStream_t stream = nullptr;
@@ -88,16 +84,13 @@ struct BatchEngine {
 
     cudaError_t enqueue(uint64_t n, int sh, unsigned g, unsigned gr)
     {
-        cudaError_t e = cudaMemsetAsync(sync, 0, sync_bytes, stream);
+        cudaError_t e = cudaMemsetAsync(sync, 0, sphb::sync_bytes(gr / g), stream);
         if (e != cudaSuccess) return e;
         BatchArgs A;
         A.boxes = table;
         A.nbox = (unsigned)boxes.size();
         A.order = order;
-        A.next = reinterpret_cast<unsigned *>(sync);
-        A.abort = reinterpret_cast<int *>(sync + 4);
-        A.any_err = reinterpret_cast<int *>(sync + 8);
-        A.groups = reinterpret_cast<GroupSync *>(sync + kSyncHeader);
+        set_sync_args(A, sync);
         A.group_size = g;
         A.nsteps = (unsigned)n;
         return persistent_launch(prec, model, sh, A, gr,
@@ -281,7 +274,7 @@ int batch_open(int nbox, const char *const *paths, const void *const *bufs, cons
     const size_t nb = B->boxes.size();
     B->table = B->alloc<sphb::BoxRec>(nb);
     B->order = B->alloc<unsigned>(nb);
-    B->sync_bytes = sphb::kSyncHeader + sizeof(sphb::GroupSync) * (size_t)B->sms * 32;
+    B->sync_bytes = sphb::sync_bytes((unsigned)B->sms * 32);
     B->sync = B->alloc<unsigned char>(B->sync_bytes);
     if (!B->table || !B->order || !B->sync) {
         g_batch_open_error = "device allocation failed";

@@ -10,6 +10,7 @@
 // maximum is reduced on the device every iteration, and the reference's
 // stopping rule (checked after iteration 0 and every 10th iteration) is
 // applied on the device -- no host round trip per check.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -17,6 +18,7 @@
 
 #include "engine_internal.h"
 #include "dem_device.cuh"
+#include "warmstart.h"
 #include "../../include/sphere_b200.h"
 
 namespace sphb {
@@ -41,6 +43,10 @@ struct DarcyCtl {
     int final_buf;                 // buffer holding the final pressure (0: p, 1: p2)
     unsigned barrier_count, barrier_gen;
     int err;
+    // learned warm start: first-iteration residuals of the previous-step
+    // guess (0) and of the network's guess (1); solves that used the latter
+    unsigned long long guess_res[2];
+    long long ws_picked;
 };
 
 struct DarcyDev {
@@ -54,6 +60,10 @@ struct DarcyDev {
     DarcyCtl *ctl;
     double host_wall0_w;
     long long conv_iters_last;
+    // learned warm start (null when off)
+    WarmStart *ws = nullptr;
+    unsigned char *freec = nullptr;        // cells the solve may change
+    double *guess = nullptr;               // padded network guess
 };
 
 __device__ __forceinline__ unsigned didx(const DarcyParams &D, int x, int y, int z)
@@ -544,6 +554,59 @@ __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, do
     }
 }
 
+// Cells whose pressure the solve may change: dp_of's zeroing conditions
+// (Dirichlet faces, cells at or above the top wall, fixed-pressure cells)
+// are false.
+__global__ void k_free_cells(DarcyParams D, const DarcyCtl *ctl, const int *p_constant,
+                             unsigned char *freec)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    const unsigned wall0_iz = ctl->wall0_iz;
+    const bool fixed = (D.bc_bot == 0 && z == 0) || (D.bc_top == 0 && z == D.nz - 1) ||
+                       ((unsigned)z >= wall0_iz && D.bc_top == 0) || (D.bc_xn == 0 && x == 0) ||
+                       (D.bc_xp == 0 && x == D.nx - 1) || (D.bc_yn == 0 && y == 0) ||
+                       (D.bc_yp == 0 && y == D.nx - 1) || p_constant[didx(D, x, y, z)] == 1;
+    freec[(size_t)(z * D.ny + y) * D.nx + x] = fixed ? 0 : 1;
+}
+
+// max |residual| of the first Jacobi iteration started from pg
+__global__ void k_guess_residual(DarcyParams D, DarcyFields F, const double *pg, DarcyCtl *ctl,
+                                 double dt, int slot)
+{
+    int x, y, z;
+    double a = 0.0;
+    if (cell_of_thread(D, x, y, z)) {
+        const unsigned c = didx(D, x, y, z);
+        const double dp_impl = dp_of(D, F, pg, ctl->wall0_iz, dt, x, y, z);
+        const double p = pg[c];
+        double p_new = F.p_old[c] + 0.5 * F.dp_expl[c] + 0.5 * dp_impl;
+        p_new = p * 0.95 + p_new * 0.05;
+        a = fabs((p_new - p) / (p + 1.0e-16));
+        if (a != a) a = 1.0e300;
+    }
+    for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+    if ((threadIdx.x & 31) == 0)
+        atomicMax(&ctl->guess_res[slot], (unsigned long long)__double_as_longlong(a));
+}
+
+// the network's guess replaces the previous-step guess only when its first
+// residual is smaller
+__global__ void k_take_guess(DarcyCtl *ctl, double *p, const double *guess, size_t ng)
+{
+    if (!(ctl->guess_res[1] < ctl->guess_res[0])) return;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < ng;
+         i += (size_t)gridDim.x * blockDim.x)
+        p[i] = guess[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ws_picked += 1;
+}
+
+__global__ void k_clear_guess_res(DarcyCtl *ctl)
+{
+    ctl->guess_res[0] = 0ull;
+    ctl->guess_res[1] = 0ull;
+}
+
 // findDarcyVelocities, darcy.cuh:1839-1897
 __global__ void k_velocities(DarcyParams D, const double *p, const double *phi, const double *k,
                              double *v)
@@ -653,6 +716,13 @@ int Engine::darcy_init()
     jacobi_grid = sms * (per_sm < 4 ? per_sm : 4);
     unsigned need = cells_blocks(D);
     if ((unsigned)jacobi_grid > need) jacobi_grid = (int)need;
+    if (warm_start) {
+        Dd.freec = dalloc<unsigned char>(nx * ny * nz);
+        Dd.guess = dalloc<double>(ng);
+        Dd.ws = ws_create(D.nx, D.ny, D.nz, 0x5eed5eedull, warm_start_train);
+        if (!Dd.ws || !Dd.freec || !Dd.guess)
+            return fail(ST_CUDA, "could not set up the learned warm start");
+    }
     return darcy_sync_wall();
 }
 
@@ -676,6 +746,7 @@ void Engine::darcy_set_host_wall()
 
 void Engine::darcy_free()
 {
+    if (darcy && darcy->ws) ws_destroy(darcy->ws);
     delete darcy;   // device arrays are released with the engine's allocations
     darcy = nullptr;
 }
@@ -715,6 +786,22 @@ cudaError_t Engine::enqueue_fluid()
     DarcyFields F{Dd.phi, Dd.dphi, Dd.k, Dd.vp_avg, Dd.p_old, Dd.dp_expl, Dd.p_constant};
     k_first_solution<<<cb, 256, 0, stream>>>(D, F, Dd.p, Dd.dp_expl, Dd.ctl, P.dt);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (Dd.ws) {
+        // learned initial iterate; the previous-step guess stays unless the
+        // network's has the smaller first residual
+        k_free_cells<<<cb, 256, 0, stream>>>(D, Dd.ctl, Dd.p_constant, Dd.freec);
+        if ((e = cudaMemcpyAsync(Dd.guess, Dd.p, Dd.ng * 8, cudaMemcpyDeviceToDevice, stream)) != cudaSuccess)
+            return e;
+        WSDarcyInputs in{Dd.p, Dd.phi, Dd.dphi, Dd.freec};
+        if ((e = ws_predict(Dd.ws, in, Dd.guess, stream)) != cudaSuccess) return e;
+        k_ghost<1><<<cb, 256, 0, stream>>>(D, Dd.guess);
+        k_clear_guess_res<<<1, 1, 0, stream>>>(Dd.ctl);
+        k_guess_residual<<<cb, 256, 0, stream>>>(D, F, Dd.p, Dd.ctl, P.dt, 0);
+        k_guess_residual<<<cb, 256, 0, stream>>>(D, F, Dd.guess, Dd.ctl, P.dt, 1);
+        k_take_guess<<<(unsigned)std::min<size_t>((Dd.ng + 255) / 256, 1024), 256, 0, stream>>>(
+            Dd.ctl, Dd.p, Dd.guess, Dd.ng);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     // the second buffer starts as a copy (its ghost faces are read too)
     if ((e = cudaMemcpyAsync(Dd.p2, Dd.p, Dd.ng * 8, cudaMemcpyDeviceToDevice, stream)) != cudaSuccess)
         return e;
@@ -725,6 +812,7 @@ cudaError_t Engine::enqueue_fluid()
     e = cudaLaunchCooperativeKernel((void *)k_jacobi, dim3(jacobi_grid), dim3(256), args, 0, stream);
     if (e != cudaSuccess) return e;
     k_final_pressure<<<cb, 256, 0, stream>>>(D, Dd.ctl, Dd.p, Dd.p2, Dd.ng);
+    if (Dd.ws && (e = ws_train(Dd.ws, Dd.p_old, Dd.p, stream)) != cudaSuccess) return e;
     if (!darcy_keep_dphi) k_zero_interior<<<cb, 256, 0, stream>>>(D, Dd.dphi);
     k_ghost<1><<<cb, 256, 0, stream>>>(D, Dd.p);
     k_velocities<<<cb, 256, 0, stream>>>(D, Dd.p, Dd.phi, Dd.k, Dd.v);
@@ -742,6 +830,7 @@ int64_t Engine::darcy_field_bytes(int f) const
     case SPH_F_DARCY_F_P: return (int64_t)hs.np * 32;
     case SPH_F_DARCY_ITERS: case SPH_F_DARCY_ITERS_TOTAL: case SPH_F_DARCY_ITERS_EXACT:
         return 8;
+    case SPH_F_DARCY_WARM: return 32;
     default: return -1;
     }
 }
@@ -766,6 +855,24 @@ int Engine::darcy_get(int f, void *dst, size_t bytes)
     case SPH_F_DARCY_F_P:
         e = cudaMemcpyAsync(dst, Dd.f_p, (size_t)need, cudaMemcpyDeviceToHost, stream);
         break;
+    case SPH_F_DARCY_WARM: {
+        // predictions, training steps, solves that used the network's guess,
+        // last training loss (as double bits)
+        DarcyCtl c;
+        e = cudaMemcpyAsync(&c, Dd.ctl, sizeof c, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "get");
+        long long v[4] = {0, 0, 0, 0};
+        if (Dd.ws) {
+            v[0] = ws_predictions(Dd.ws);
+            v[1] = ws_trained(Dd.ws);
+            v[2] = c.ws_picked;
+            double loss = ws_last_loss(Dd.ws, stream);
+            std::memcpy(&v[3], &loss, 8);
+        }
+        std::memcpy(dst, v, 32);
+        return ST_OK;
+    }
     default: {
         DarcyCtl c;
         e = cudaMemcpyAsync(&c, Dd.ctl, sizeof c, cudaMemcpyDeviceToHost, stream);

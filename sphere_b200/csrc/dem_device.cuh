@@ -382,7 +382,7 @@ __device__ __forceinline__ int pick_slot(uint64_t mask, uint64_t full, const uin
 struct ContactOut {
     V3 F, T;
     double es_dot, ev_dot, p;
-    double wf[5];   // force on each dynamic wall (walls_force_pp)
+    double wf0, wf1, wf2, wf3, wf4;   // force on each dynamic wall (walls_force_pp)
 };
 
 // Contact search + forces of sorted particle k (topology and interact of
@@ -533,45 +533,50 @@ __device__ __forceinline__ bool contact_particle(const DevParams &P, const DevSt
     }
 
     // --- walls (contactsearch.cuh:602-701) ---
-    double4 wnx[5] = {make_double4(0.0f, 0.0f, -1.0f, P.L[2]), make_double4(-1.0f, 0.0f, 0.0f, P.L[0]),
-                      make_double4(1.0f, 0.0f, 0.0f, 0.0f), make_double4(0.0f, -1.0f, 0.0f, P.L[1]),
-                      make_double4(0.0f, 1.0f, 0.0f, 0.0f)};
-    double wvel[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (unsigned w = 0; w < P.nw && w < 5; ++w) {
-        wnx[w] = S.wnx[w];
-        wvel[w] = S.wmvfd[w].y;
-    }
-    double wf[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    // walls beyond nw keep the reference's defaults (the domain faces); the
+    // five walls are unrolled so their state stays in registers
+    const unsigned nw = P.nw;
+    const double4 wnx0 = nw > 0 ? S.wnx[0] : make_double4(0.0f, 0.0f, -1.0f, P.L[2]);
+    const double4 wnx1 = nw > 1 ? S.wnx[1] : make_double4(-1.0f, 0.0f, 0.0f, P.L[0]);
+    const double4 wnx2 = nw > 2 ? S.wnx[2] : make_double4(1.0f, 0.0f, 0.0f, 0.0f);
+    const double4 wnx3 = nw > 3 ? S.wnx[3] : make_double4(0.0f, -1.0f, 0.0f, P.L[1]);
+    const double4 wnx4 = nw > 4 ? S.wnx[4] : make_double4(0.0f, 1.0f, 0.0f, 0.0f);
+    double wf0 = 0.0, wf1 = 0.0, wf2 = 0.0, wf3 = 0.0, wf4 = 0.0;
     V3 vlin = xyz(vel_a);
-    double dw = wnx[0].w - (xa.z + ra);
+    double dw = wnx0.w - (xa.z + ra);
     if (dw < 0.0f)
-        wf[0] = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx[0]), dw, wvel[0]);
+        wf0 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx0), dw,
+                             nw > 0 ? S.wmvfd[0].y : 0.0);
     dw = xa.z - ra - P.origo[2];
     if (dw < 0.0f)
         (void)wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a,
                                  mk3(0.0f, 0.0f, 1.0f), dw, 0.0);
     if (P.periodic == 0) {
-        dw = wnx[1].w - (xa.x + ra);
+        dw = wnx1.w - (xa.x + ra);
         if (dw < 0.0f)
-            wf[1] = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx[1]), dw, wvel[1]);
-        dw = xa.x - ra - wnx[2].w;
+            wf1 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx1), dw,
+                                 nw > 1 ? S.wmvfd[1].y : 0.0);
+        dw = xa.x - ra - wnx2.w;
         if (dw < 0.0f)
-            wf[2] = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx[2]), dw, wvel[2]);
+            wf2 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx2), dw,
+                                 nw > 2 ? S.wmvfd[2].y : 0.0);
     }
     if (P.periodic == 0 || P.periodic == 2) {
-        dw = wnx[3].w - (xa.y + ra);
+        dw = wnx3.w - (xa.y + ra);
         if (dw < 0.0f)
-            wf[3] = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx[3]), dw, wvel[3]);
-        dw = xa.y - ra - wnx[4].w;
+            wf3 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx3), dw,
+                                 nw > 3 ? S.wmvfd[3].y : 0.0);
+        dw = xa.y - ra - wnx4.w;
         if (dw < 0.0f)
-            wf[4] = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx[4]), dw, wvel[4]);
+            wf4 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx4), dw,
+                                 nw > 4 ? S.wmvfd[4].y : 0.0);
     }
     out.F = F;
     out.T = T;
     out.es_dot = es_dot;
     out.ev_dot = ev_dot;
     out.p = p;
-    for (int w = 0; w < 5; ++w) out.wf[w] = wf[w];
+    out.wf0 = wf0; out.wf1 = wf1; out.wf2 = wf2; out.wf3 = wf3; out.wf4 = wf4;
     return true;
 }
 
@@ -587,7 +592,12 @@ __device__ __forceinline__ void contact_writeback(const DevParams &P, const DevS
     S.es[k] += c.es_dot * P.dt;
     S.ev[k] += c.ev_dot * P.dt;
     S.p[k] = c.p;
-    for (unsigned w = 0; w < P.nw && w < 5; ++w) S.walls_force_pp[o + (size_t)P.np * w] = c.wf[w];
+    const size_t np = P.np;
+    if (P.nw > 0) S.walls_force_pp[o] = c.wf0;
+    if (P.nw > 1) S.walls_force_pp[o + np] = c.wf1;
+    if (P.nw > 2) S.walls_force_pp[o + 2 * np] = c.wf2;
+    if (P.nw > 3) S.walls_force_pp[o + 3 * np] = c.wf3;
+    if (P.nw > 4) S.walls_force_pp[o + 4 * np] = c.wf4;
 }
 
 // 6 resident blocks of 128 threads per SM (80 registers): measured best

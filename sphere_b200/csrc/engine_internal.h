@@ -34,6 +34,7 @@ public:
     int verbose = 0;
     int graph_steps = 64;
     int warm_start = 0;
+    int warm_start_train = 2000;  // solves the warm-start network trains on
     int step_kernel = 0;          // 0 automatic, 1 per-stage kernels, 2 persistent
     std::string outdir = "output";
     std::string sid = "unnamed";

@@ -27,9 +27,6 @@ struct PersistDev {
 
 namespace {
 
-// layout of the sync block: [next u32][abort i32][any_err i32][pad][GroupSync ...]
-constexpr size_t kSyncHeader = 16;
-
 __global__ void k_refresh_f(DevParams P, DevState S)
 {
     unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -77,8 +74,8 @@ int Engine::persist_init()
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&D.sms, cudaDevAttrMultiProcessorCount, dev);
-    // at most one group per block of the largest grid
-    D.sync_bytes = kSyncHeader + sizeof(GroupSync) * (size_t)D.sms * 32;
+    // one group: the whole grid steps the box
+    D.sync_bytes = sync_bytes(1);
     D.sync = dalloc<unsigned char>(D.sync_bytes);
     if (!D.pc || !D.table || !D.order || !D.sync) return fail(ST_CUDA, "device allocation failed");
     BoxRec r;
@@ -131,10 +128,7 @@ cudaError_t Engine::persist_launch(uint64_t n, int shape, unsigned grid)
     A.boxes = D.table;
     A.nbox = 1;
     A.order = D.order;
-    A.next = reinterpret_cast<unsigned *>(D.sync);
-    A.abort = reinterpret_cast<int *>(D.sync + 4);
-    A.any_err = reinterpret_cast<int *>(D.sync + 8);
-    A.groups = reinterpret_cast<GroupSync *>(D.sync + kSyncHeader);
+    set_sync_args(A, D.sync);
     A.group_size = grid;
     A.nsteps = (unsigned)n;
     return persistent_launch(precision, (int)hs.contactmodel, shape, A, grid,

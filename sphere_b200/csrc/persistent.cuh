@@ -64,10 +64,19 @@ struct BoxRec {
     unsigned pad;
 };
 
+// Barrier state of one group: the arrival counter and the generation the
+// waiters poll sit on different 128-byte lines.  Groups of more than 64
+// blocks arrive through 16 sub-counters first (sub[], one line each).
 struct GroupSync {
-    unsigned count, gen;
+    unsigned count;
     int box;
-    int pad;
+    unsigned pad0[30];
+    unsigned gen;
+    unsigned pad1[31];
+};
+constexpr int kBarrierSubs = 16;
+struct GroupTree {
+    unsigned sub[kBarrierSubs][32];
 };
 
 struct BatchArgs {
@@ -76,6 +85,7 @@ struct BatchArgs {
     const unsigned *order;     // processing order (largest box first)
     unsigned *next;            // work counter, zero at launch
     GroupSync *groups;         // zero at launch
+    GroupTree *tree;           // zero at launch; sub-counters of group 0
     unsigned group_size;
     unsigned nsteps;
     int *abort;                // set when a barrier gave up; every group stops
@@ -84,8 +94,11 @@ struct BatchArgs {
 
 // Barrier over the blocks of one group, bounded: after ~2^24 polls it sets
 // *abort and returns false, and every waiting block returns false as soon
-// as it sees *abort.
-__device__ __forceinline__ bool group_barrier(GroupSync *g, unsigned size, int *abort)
+// as it sees *abort.  Groups of more than 64 blocks (only ever group 0: a
+// single box stepped by the whole grid) arrive in two levels so no counter
+// takes more than ~64 serialised atomics.
+__device__ __forceinline__ bool group_barrier(GroupSync *g, GroupTree *tree, unsigned size,
+                                              unsigned rank, int *abort)
 {
     if (size == 1) {
         __syncthreads();
@@ -97,14 +110,26 @@ __device__ __forceinline__ bool group_barrier(GroupSync *g, unsigned size, int *
         volatile unsigned *gen = &g->gen;
         const unsigned cur = *gen;
         __threadfence();
-        const unsigned arrived = atomicAdd(&g->count, 1u);
+        bool last;
+        if (size > 64) {
+            const unsigned s = rank % kBarrierSubs;
+            const unsigned members = (size - s + kBarrierSubs - 1) / kBarrierSubs;
+            last = false;
+            if (atomicAdd(&tree->sub[s][0], 1u) == members - 1) {
+                tree->sub[s][0] = 0;
+                __threadfence();
+                last = atomicAdd(&g->count, 1u) == kBarrierSubs - 1;
+            }
+        } else {
+            last = atomicAdd(&g->count, 1u) == size - 1;
+        }
         ok = 1;
-        if (arrived == size - 1) {
+        if (last) {
             g->count = 0;
             __threadfence();
             atomicAdd(&g->gen, 1u);
         } else {
-            unsigned spins = 0;
+            unsigned spins = 0, nap = 32;
             while (*gen == cur) {
                 if (++spins > (1u << 24)) {
                     atomicExch(abort, 1);
@@ -115,7 +140,8 @@ __device__ __forceinline__ bool group_barrier(GroupSync *g, unsigned size, int *
                     ok = 0;
                     break;
                 }
-                __nanosleep(16);
+                __nanosleep(nap);
+                if (nap < 256) nap <<= 1;
             }
         }
         __threadfence();
@@ -136,14 +162,20 @@ __global__ void __launch_bounds__(NT, MINB) k_persistent(BatchArgs A)
     __shared__ BoxRec box;
     __shared__ double cache[256];
     __shared__ StepHead h;
-    __shared__ int s_box, s_last;
+    __shared__ int s_box;
+    // this block's copy of the walls: every block moves them identically
+    // from the same partial sums, block 0 of the group publishes them
+    __shared__ double4 sw_nx[6], sw_mvfd[6];
+    __shared__ double sw_acc[6];
+    __shared__ double4 *g_wnx, *g_wmvfd;
+    __shared__ double *g_wacc;
 
     const unsigned gsz = A.group_size;
     const unsigned gid = blockIdx.x / gsz, rank = blockIdx.x % gsz;
     GroupSync *G = &A.groups[gid];
     const unsigned B = blockDim.x, t = threadIdx.x;
     const unsigned gtid = rank * B + t, gstride = gsz * B;
-    auto bar = [&]() { return group_barrier(G, gsz, A.abort); };
+    auto bar = [&]() { return group_barrier(G, A.tree, gsz, rank, A.abort); };
 
     for (;;) {
         // ---- take the next box ----
@@ -161,18 +193,37 @@ __global__ void __launch_bounds__(NT, MINB) k_persistent(BatchArgs A)
             uint32_t *dst = reinterpret_cast<uint32_t *>(&box);
             for (unsigned i = t; i < sizeof(BoxRec) / 4; i += B) dst[i] = src[i];
         }
+        __syncthreads();
         if (t == 0) {
             // the loop state as the host (or the last launch) left it;
             // nothing writes it before this box's first W phase
-            const DevCtl *ctl = A.boxes[bi].S[0].ctl;
-            const PersistCtl *pc = A.boxes[bi].pc;
+            const DevCtl *ctl = box.S[0].ctl;
             h.iter = *(volatile long long *)&ctl->iter;
             h.t_current = *(volatile double *)&ctl->t_current;
             h.velocity_state = *(volatile int *)&ctl->velocity_state;
             h.err = *(volatile int *)&ctl->err;
             h.resort = *(volatile int *)&ctl->resort;
             h.nl = *(volatile int *)&ctl->nl_rebuild;
-            h.view = *(volatile int *)&pc->view;
+            h.view = *(volatile int *)&box.pc->view;
+            g_wnx = box.S[0].wnx;
+            g_wmvfd = box.S[0].wmvfd;
+            g_wacc = box.S[0].wacc;
+            for (unsigned w = 0; w < box.P.nw && w < 6; ++w) {
+                sw_nx[w] = ldcg4(&g_wnx[w]);
+                sw_mvfd[w] = ldcg4(&g_wmvfd[w]);
+                sw_acc[w] = __ldcg(&g_wacc[w]);
+            }
+            for (int v = 0; v < 2; ++v) {
+                box.S[v].wnx = sw_nx;
+                box.S[v].wmvfd = sw_mvfd;
+                box.S[v].wacc = sw_acc;
+            }
+            if (rank == 0) {
+                // flags a previous launch left behind were carried into ctl
+                PersistCtl *pc = box.pc;
+                pc->flag_resort[0] = pc->flag_resort[1] = 0;
+                pc->flag_nl[0] = pc->flag_nl[1] = 0;
+            }
         }
         // every block has read the loop state before any block changes it
         if (!bar()) return;
@@ -180,26 +231,14 @@ __global__ void __launch_bounds__(NT, MINB) k_persistent(BatchArgs A)
         PersistCtl *pc = box.pc;
 
         for (unsigned s = 0; s < A.nsteps; ++s) {
-            if (s > 0) {
-                // published by the previous step's finalizer before the barrier
-                if (t == 0) {
-                    const volatile StepHead *src = &pc->head[(h.iter) & 1];
-                    h.t_current = src->t_current;
-                    h.velocity_state = src->velocity_state;
-                    h.err = src->err;
-                    h.resort = src->resort;
-                    h.nl = src->nl;
-                    h.view = src->view;
-                }
-                __syncthreads();
-            }
             if (h.err) break;
             const int v = h.view;
             const DevState &S = box.S[v];
             const long long iter = h.iter;
             bool nl = h.nl != 0;
+            const bool resorted = h.resort != 0;
             // ---- re-sort ----
-            if (h.resort) {
+            if (resorted) {
                 PermScratch W = make_perm_scratch(box.scratch, P.np);
                 if (!resort_group(P, S, W, gsz, rank, bar, PREC == 2)) {
                     if (t == 0) raise_err(S.ctl, DERR_TIMEOUT, -1);
@@ -225,52 +264,54 @@ __global__ void __launch_bounds__(NT, MINB) k_persistent(BatchArgs A)
                                    S.angvel_nx, S.vel_f_nx, S.angvel_f_nx, fr, fn);
             }
             if (!bar()) return;
-            // ---- W: wall-force partials; the last block finishes the step ----
-            if (P.nw > 0 && P.np > 0)
+            // ---- W: wall-force partials ----
+            // the previous step's flags: every block read them before this barrier
+            if (rank == 0 && t == 0) {
+                pc->flag_resort[(iter + 1) & 1] = 0;
+                pc->flag_nl[(iter + 1) & 1] = 0;
+            }
+            if (P.nw > 0)
                 for (unsigned j = rank; j < box.nblk; j += gsz) {
                     double sj = chunk_tree_sum(S.walls_force_pp, P.np, j, cache);
                     if (t == 0) S.partials[j] = sj;
                 }
+            if (!bar()) return;
+            // ---- every block: ordered wall sum, walls, clock, next flags ----
+            double wforce = P.nw > 0 ? ordered_sum(S.partials, box.nblk, stage) : 0.0;
             if (t == 0) {
-                __threadfence();
-                s_last = atomicAdd(&pc->ticket, 1u) == gsz - 1;
-            }
-            __syncthreads();
-            if (s_last) {
-                __threadfence();
-                double wforce = (P.nw > 0 && P.np > 0) ? ordered_sum(S.partials, box.nblk, stage) : 0.0;
-                if (t == 0) {
-                    DevCtl *ctl = S.ctl;
-                    walls_integrate(P, S, wforce, iter, h.t_current);
-                    StepHead nh;
-                    nh.iter = iter + 1;
-                    nh.t_current = h.t_current + P.dt;
-                    nh.velocity_state = next_velocity_state(h.velocity_state, h.t_current);
-                    nh.err = *(volatile int *)&ctl->err;
-                    nh.resort = *(volatile int *)fr;
-                    nh.nl = *(volatile int *)fn;
-                    nh.view = v ^ 1;
-                    nh.pad = 0;
-                    *fr = 0;
-                    *fn = 0;
-                    pc->head[(iter + 1) & 1] = nh;
-                    if (nh.err) atomicOr(A.any_err, 1);
-                    pc->view = v ^ 1;
-                    ctl->iter = nh.iter;
-                    ctl->t_current = nh.t_current;
-                    ctl->velocity_state = nh.velocity_state;
-                    // flags the host raised were consumed by this launch's
-                    // first step; the ones raised in this step carry on
-                    ctl->resort = nh.resort;
-                    ctl->nl_rebuild = nh.nl;
-                    if (h.resort) ctl->resorts += 1;
+                DevCtl *ctl = S.ctl;
+                walls_integrate(P, S, wforce, iter, h.t_current);   // this block's copies
+                const int err = *(volatile int *)&ctl->err;
+                const int nres = *(volatile int *)fr, nnl = *(volatile int *)fn;
+                const double t_next = h.t_current + P.dt;
+                const int vs_next = next_velocity_state(h.velocity_state, h.t_current);
+                if (rank == 0) {
+                    for (unsigned w = 0; w < P.nw && w < 6; ++w) {
+                        g_wnx[w] = sw_nx[w];
+                        g_wmvfd[w] = sw_mvfd[w];
+                        g_wacc[w] = sw_acc[w];
+                    }
+                    ctl->iter = iter + 1;
+                    ctl->t_current = t_next;
+                    ctl->velocity_state = vs_next;
+                    // flags the host raised were consumed by the first step;
+                    // the ones raised in this step are pending for the next
+                    ctl->resort = nres;
+                    ctl->nl_rebuild = nnl;
+                    if (resorted) ctl->resorts += 1;
                     if (nl) ctl->nl_builds += 1;
-                    pc->ticket = 0;
+                    pc->view = v ^ 1;
+                    if (err) atomicOr(A.any_err, 1);
                     __threadfence();
                 }
+                h.iter = iter + 1;
+                h.t_current = t_next;
+                h.velocity_state = vs_next;
+                h.err = err;
+                h.resort = nres;
+                h.nl = nnl;
+                h.view = v ^ 1;
             }
-            if (!bar()) return;
-            if (t == 0) h.iter = iter + 1;
             __syncthreads();
         }
     }

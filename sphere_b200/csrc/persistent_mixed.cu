@@ -33,9 +33,10 @@ template <int MODEL>
 cudaError_t launch_shape(int shape, const BatchArgs &A, unsigned grid, size_t smem, cudaStream_t st)
 {
     switch (shape) {
-    case 0: return launch_t<MODEL, 64, 12>(A, grid, smem, st);
-    case 1: return launch_t<MODEL, 128, 6>(A, grid, smem, st);
-    case 2: return launch_t<MODEL, 256, 3>(A, grid, smem, st);
+    case 0: return launch_t<MODEL, 64, 8>(A, grid, smem, st);
+    case 1: return launch_t<MODEL, 128, 4>(A, grid, smem, st);
+    case 2: return launch_t<MODEL, 256, 2>(A, grid, smem, st);
+    case 3: return launch_t<MODEL, 128, 3>(A, grid, smem, st);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -44,9 +45,10 @@ template <int MODEL>
 int occ_shape(int shape, size_t smem)
 {
     switch (shape) {
-    case 0: return occ_t<MODEL, 64, 12>(smem);
-    case 1: return occ_t<MODEL, 128, 6>(smem);
-    case 2: return occ_t<MODEL, 256, 3>(smem);
+    case 0: return occ_t<MODEL, 64, 8>(smem);
+    case 1: return occ_t<MODEL, 128, 4>(smem);
+    case 2: return occ_t<MODEL, 256, 2>(smem);
+    case 3: return occ_t<MODEL, 128, 3>(smem);
     default: return 0;
     }
 }

@@ -1,0 +1,42 @@
+// Learned warm start of the Darcy pressure solve (warmstart.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sphb {
+
+struct WarmStart;
+
+// Darcy fields the network reads, ghost-padded (nx+2)(ny+2)(nz+2) doubles,
+// and the cells the solve may change (interior, x fastest, 1 = free).
+struct WSDarcyInputs {
+    const double *p;      // previous solution
+    const double *phi, *dphi;
+    const unsigned char *free;
+};
+
+// nullptr when the device cannot run the tensor-core kernels.
+WarmStart *ws_create(int nx, int ny, int nz, uint64_t seed, int train_solves);
+void ws_destroy(WarmStart *w);
+// Network prediction for this solve: guess = p + free * predicted change
+// (interior cells of the padded guess array).
+cudaError_t ws_predict(WarmStart *w, const WSDarcyInputs &in, double *guess, cudaStream_t st);
+// One Adam step towards the solve's result p_star from p_prev (the inputs
+// of the last prediction); nothing once the training budget is spent.
+cudaError_t ws_train(WarmStart *w, const double *p_prev, const double *p_star, cudaStream_t st);
+int ws_trained(const WarmStart *w);
+int ws_predictions(const WarmStart *w);
+int ws_error(WarmStart *w, cudaStream_t st);
+float ws_last_loss(WarmStart *w, cudaStream_t st);
+
+// test hooks on host arrays: parameters of layer 0..2 (w: [27][16 out][16 in],
+// b: [16]), forward of already-normalised 3-channel inputs, and the
+// gradients of the mean squared error over free cells
+int ws_set_params(WarmStart *w, int layer, const float *wt, const float *b);
+int ws_get_params(WarmStart *w, int layer, float *wt, float *b);
+int ws_forward_host(WarmStart *w, const float *x3, float *out);
+int ws_gradients_host(WarmStart *w, const float *x3, const float *target,
+                      const unsigned char *free, float *dw, float *db);
+
+}  // namespace sphb

@@ -23,14 +23,14 @@ FIELDS = [
     "es_dot", "es", "ev_dot", "ev", "p", "cellid", "index", "cellstart", "cellend",
     "contacts", "delta_t", "distmod", "walls_nx", "walls_mvfd", "walls_acc", "iter",
     "time", "darcy_p", "darcy_phi", "darcy_dphi", "darcy_k", "darcy_v", "darcy_f_p",
-    "darcy_iters", "darcy_iters_total", "darcy_iters_exact", "bonds", "bonds_delta", "bonds_omega",
+    "darcy_iters", "darcy_iters_total", "darcy_iters_exact", "darcy_warm", "bonds", "bonds_delta", "bonds_omega",
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 _VEC4 = {"x", "vel", "angvel", "angpos", "force", "torque", "acc", "angacc", "xyzsum",
          "delta_t", "distmod", "walls_nx", "walls_mvfd", "darcy_f_p", "bonds_delta",
          "bonds_omega"}
 _U32 = {"cellid", "index", "cellstart", "cellend", "contacts", "bonds"}
-_I64 = {"iter", "darcy_iters", "darcy_iters_total", "darcy_iters_exact"}
+_I64 = {"iter", "darcy_iters", "darcy_iters_total", "darcy_iters_exact", "darcy_warm"}
 
 STATUS = {
     0: "ok", 1: "Darcy solve did not converge", -1: "file error", -2: "version",
@@ -135,6 +135,15 @@ def lib() -> ctypes.CDLL:
     L.sph_batch_last_error.argtypes = [P]
     L.sph_batch_last_error.restype = ctypes.c_char_p
     L.sph_batch_close.argtypes = [P]
+    # warm-start network
+    L.sph_wsnet_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+                                   ctypes.POINTER(P)]
+    L.sph_wsnet_set_params.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    L.sph_wsnet_get_params.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    L.sph_wsnet_forward.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p]
+    L.sph_wsnet_gradients.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p]
+    L.sph_wsnet_destroy.argtypes = [P]
     _lib = L
     return L
 
@@ -359,3 +368,61 @@ class Batch:
 
     def write_bin(self, box, path) -> None:
         self._check(lib().sph_batch_write_bin(self._h, int(box), os.fsencode(path)))
+
+
+class WSNet:
+    """The Darcy warm-start network on its own (``sph_wsnet_*``): BF16
+    tensor-core forward and backward on host arrays, for gradient checks."""
+
+    def __init__(self, nx, ny, nz, seed=1):
+        h = ctypes.c_void_p()
+        rc = lib().sph_wsnet_create(int(nx), int(ny), int(nz), int(seed), ctypes.byref(h))
+        if rc != 0:
+            raise EngineError(rc, "could not create the warm-start network")
+        self._h = h
+        self.ncells = nx * ny * nz
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().sph_wsnet_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, layer, w, b):
+        w = numpy.ascontiguousarray(w, dtype=numpy.float32)
+        b = numpy.ascontiguousarray(b, dtype=numpy.float32)
+        assert w.size == 27 * 256 and b.size == 16
+        if lib().sph_wsnet_set_params(self._h, int(layer), w.ctypes.data, b.ctypes.data):
+            raise EngineError(-4, "set_params failed")
+
+    def get_params(self, layer):
+        w = numpy.empty((27, 16, 16), dtype=numpy.float32)
+        b = numpy.empty(16, dtype=numpy.float32)
+        if lib().sph_wsnet_get_params(self._h, int(layer), w.ctypes.data, b.ctypes.data):
+            raise EngineError(-4, "get_params failed")
+        return w, b
+
+    def forward(self, x3):
+        x3 = numpy.ascontiguousarray(x3, dtype=numpy.float32)
+        out = numpy.empty(self.ncells, dtype=numpy.float32)
+        rc = lib().sph_wsnet_forward(self._h, x3.ctypes.data, out.ctypes.data)
+        if rc:
+            raise EngineError(rc, "forward failed")
+        return out
+
+    def gradients(self, x3, target, free):
+        x3 = numpy.ascontiguousarray(x3, dtype=numpy.float32)
+        target = numpy.ascontiguousarray(target, dtype=numpy.float32)
+        free = numpy.ascontiguousarray(free, dtype=numpy.uint8)
+        dw = numpy.empty((3, 27, 16, 16), dtype=numpy.float32)
+        db = numpy.empty((3, 16), dtype=numpy.float32)
+        rc = lib().sph_wsnet_gradients(self._h, x3.ctypes.data, target.ctypes.data,
+                                       free.ctypes.data, dw.ctypes.data, db.ctypes.data)
+        if rc:
+            raise EngineError(rc, "gradients failed")
+        return dw, db
