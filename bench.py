@@ -253,6 +253,9 @@ def run_gpu(args):
                                   "bonds": prof.bonds_ms, "integrate": prof.integrate_ms,
                                   "step": prof.step_ms},
         "resorts": int(info.resorts),
+        "step_path": {"kernel": "persistent" if info.step_path == 1 else "per-stage",
+                      "threads": int(info.step_threads), "grid": int(info.step_grid),
+                      "autotuned": bool(info.tuned)},
         "clocks": clocks,
     }
     if plain is not None:
@@ -262,7 +265,88 @@ def run_gpu(args):
         out["force_rel_err_vs_fp64"] = force_error(d)
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(d, sample_steps=args.cpu_steps)
+    if args.darcy_steps > 0:
+        out["darcy"] = darcy_leg(args)
+    if args.batch_boxes > 0:
+        out["batch"] = batch_leg(args)
     return out
+
+
+def darcy_leg(args):
+    """Darcy-coupled consolidation (40 x 40 x 80 fluid grid, residual
+    tolerance 1e-8, top wall stepped 10 -> 20 -> 40 -> 80 kPa): Jacobi
+    iterations per fluid step without and with the learned warm start.  The
+    network trains online from the first solve; the comparison uses the
+    second half of the steps, exact iteration counts (the first iteration
+    whose residual met the tolerance) and the reference's own count (checks
+    every 10 iterations)."""
+    from sphere_b200 import configs
+    from sphere_b200.engine import Engine
+    d = configs.darcy_benchmark(n=args.particles, seed=SEED, log=log)
+    steps = args.darcy_steps
+    loads = [10e3, 20e3, 40e3, 80e3]
+    arms = {}
+    for warm in (False, True):
+        eng = Engine(d, fluid=True, precision="mixed", warm_start=warm)
+        mv = eng.get("walls_mvfd")
+        exact, quant, ms = [], [], []
+        for s in range(steps):
+            load = loads[min(len(loads) - 1, s * len(loads) // steps)]
+            if mv[0, 3] != load:
+                mv[0, 3] = load
+                eng.set("walls_mvfd", mv)
+            ms.append(eng.step_timed(1))
+            exact.append(int(eng.get("darcy_iters_exact")[0]))
+            quant.append(int(eng.get("darcy_iters")[0]) + 1)
+        stats = eng.get("darcy_warm")
+        eng.close()
+        h = steps // 2
+        arms["warm" if warm else "plain"] = {
+            "iters_exact_per_step": float(numpy.mean(exact[h:])),
+            "iters_per_step": float(numpy.mean(quant[h:])),
+            "ms_per_fluid_step": float(numpy.mean(ms[h:])),
+            "predictions": int(stats[0]), "trained": int(stats[1]), "used_network_guess": int(stats[2]),
+        }
+        log(f"darcy {'warm' if warm else 'plain'}: {arms['warm' if warm else 'plain']}")
+    p, w = arms["plain"], arms["warm"]
+    return {
+        "workload": f"Darcy consolidation, N={d.np}, fluid grid {int(d.num[0])}x{int(d.num[1])}x{int(d.num[2])}, "
+                    "mu_f=1.797e-6 Pa s, k_c=3.5e-13 m^2, beta_f=4.5e-10 1/Pa, tolerance 1e-8, "
+                    "top wall 10->20->40->80 kPa",
+        "steps": steps, "measured_steps": steps - steps // 2,
+        "iters_per_step_plain": p["iters_exact_per_step"],
+        "iters_per_step_warm": w["iters_exact_per_step"],
+        "iteration_reduction": p["iters_exact_per_step"] / max(w["iters_exact_per_step"], 1e-9),
+        "plain": p, "warm": w,
+    }
+
+
+def batch_leg(args):
+    """The batched ensemble: independent shear boxes (particle counts
+    log-uniform in [2000, 20000]) stepped by one persistent launch per call,
+    launch shape from the autotuner, replayed as a CUDA graph."""
+    from sphere_b200 import configs
+    from sphere_b200.engine import Batch
+    boxes, meta = configs.batch_shear_boxes(nbox=args.batch_boxes, seed=7)
+    total = int(sum(m["n"] for m in meta))
+    interval = 100
+    with Batch(boxes, precision="mixed") as b:
+        b.step(300)                      # autotunes on its first steps
+        for _ in range(2):
+            b.step(interval)             # captures the graph
+        times = [b.step_timed(interval) for _ in range(args.batch_steps)]
+        cfg = b.config()
+        trials = b.trials()
+    step_s = float(numpy.sum(times)) * 1e-3
+    return {
+        "workload": f"{len(boxes)} shear boxes, {total} particles (counts log-uniform in [2000, 20000]), "
+                    "radii U(0.009, 0.011) m, sigma0 in {10..160} kPa, shear U(1e-5, 1e-3) m/s, "
+                    "k_n = k_t = 1.16e7 N/m, mu U(0.3, 0.6), mixed precision",
+        "particle_steps_per_s": total * interval * len(times) / step_s,
+        "ms_per_step": 1e3 * step_s / len(times), "dem_steps_per_step": interval,
+        "launch": cfg, "autotuner_trials": len(trials),
+        "best_trial_ms_per_step": min(t["ms_per_step"] for t in trials) if trials else None,
+    }
 
 
 def cpu_baseline(d, sample_steps=3):
@@ -341,6 +425,11 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--ref-sample", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--darcy-steps", type=int, default=200,
+                    help="fluid steps per arm of the Darcy leg (0 skips it)")
+    ap.add_argument("--batch-boxes", type=int, default=256,
+                    help="boxes of the batched-ensemble leg (0 skips it)")
+    ap.add_argument("--batch-steps", type=int, default=5)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

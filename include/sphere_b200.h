@@ -118,6 +118,10 @@ typedef struct sph_info {
     double time, time_total, dt, file_dt;
     uint32_t step_count;
     int64_t resorts;      /* re-sorts performed (steps where a particle changed cell) */
+    int32_t step_path;    /* 0 per-stage kernels, 1 fused persistent step */
+    int32_t step_threads; /* persistent path: threads per block chosen by the autotuner */
+    int32_t step_grid;    /* persistent path: blocks of the launch */
+    int32_t tuned;        /* 1 once the autotuner has run */
 } sph_info;
 
 /* Fills *opts with the defaults (faithful FP64, TY3, 32 slots, device -1). */

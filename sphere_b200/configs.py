@@ -320,13 +320,9 @@ def settle_packing(n: int = 100000, seed: int = 1, r_min: float = 0.008,
     return state
 
 
-def shear_benchmark(n: int = 100000, seed: int = 1, sigma0: float = 20e3,
-                    shear_velocity: float = 1e-4, cache_dir=None, log=None) -> BinData:
-    """The dense-shear workload: a settled packing of n spheres (radii
-    U(0.008, 0.012) m), fixed bottom layer, top layer sheared at
-    shear_velocity along x, one top wall at normal stress sigma0, Young's
-    modulus contact E = 7e8 Pa, mu = 0.5, periodic x/y.  The settled packing
-    is cached as a .bin file under cache_dir."""
+def settled_packing(n: int = 100000, seed: int = 1, cache_dir=None, log=None) -> BinData:
+    """The settled packing of the benchmark workloads (cached as a .bin file
+    under cache_dir, default $SPHB_CACHE or /tmp/sphere_b200_cache)."""
     import os
     from .binfile import read_bin, write_bin
 
@@ -334,12 +330,51 @@ def shear_benchmark(n: int = 100000, seed: int = 1, sigma0: float = 20e3,
     os.makedirs(cache_dir, exist_ok=True)
     path = os.path.join(cache_dir, f"packing4_n{n}_seed{seed}.bin")
     if os.path.exists(path):
-        base = read_bin(path)
-    else:
-        base = settle_packing(n=n, seed=seed, log=log)
-        write_bin(base, path + ".tmp")
-        os.replace(path + ".tmp", path)
-    d = base.copy()
+        return read_bin(path)
+    base = settle_packing(n=n, seed=seed, log=log)
+    write_bin(base, path + ".tmp")
+    os.replace(path + ".tmp", path)
+    return base
+
+
+def darcy_benchmark(n: int = 100000, seed: int = 1, grid=(40, 40, 80), sigma0: float = 10e3,
+                    cache_dir=None, log=None) -> BinData:
+    """The Darcy-coupled consolidation workload: the settled packing on a
+    40 x 40 x 80 fluid (and sorting) grid, a stress-controlled top wall at
+    sigma0 (the benchmark steps it 10 -> 20 -> 40 -> 80 kPa), Young's modulus
+    E = 7e8 Pa, mu = 0.5, Darcy flow with mu_f = 1.797e-6 Pa s, rho_f = 1000
+    kg/m^3, k_c = 3.5e-13 m^2, beta_f = 4.5e-10 1/Pa, residual tolerance
+    1e-8, bottom no-flow, top Dirichlet, periodic sides."""
+    d = settled_packing(n, seed, cache_dir, log).copy()
+    default_params(d, mu_s=0.5, mu_d=0.5, k_n=1.16e7, k_t=1.16e7)
+    d.E = 7e8
+    d.gamma_wn = 1.0e4
+    d.gamma_wt = 0.0
+    nx, ny, nz = grid
+    dx = float(d.L[0]) / nx
+    d.origo = numpy.zeros(3)
+    d.L = numpy.array([nx * dx, ny * dx, nz * dx])
+    d.num = numpy.array([nx, ny, nz], dtype=numpy.uint32)
+    d.vel[:] = 0.0
+    d.angvel[:] = 0.0
+    add_top_wall(d, sigma0, wmode=1)
+    d.time_dt = time_step(d)
+    d.time_current = 0.0
+    d.time_total = 1e9 * d.time_dt
+    d.time_file_dt = d.time_total
+    init_fluid_darcy(d, mu=1.797e-6, rho_f=1000.0, k_c=3.5e-13, beta_f=4.5e-10,
+                     tolerance=1e-8, maxiter=200000, bottom_no_flow=True)
+    return d
+
+
+def shear_benchmark(n: int = 100000, seed: int = 1, sigma0: float = 20e3,
+                    shear_velocity: float = 1e-4, cache_dir=None, log=None) -> BinData:
+    """The dense-shear workload: a settled packing of n spheres (radii
+    U(0.008, 0.012) m), fixed bottom layer, top layer sheared at
+    shear_velocity along x, one top wall at normal stress sigma0, Young's
+    modulus contact E = 7e8 Pa, mu = 0.5, periodic x/y.  The settled packing
+    is cached as a .bin file under cache_dir."""
+    d = settled_packing(n, seed, cache_dir, log).copy()
     default_params(d, mu_s=0.5, mu_d=0.5, k_n=1.16e7, k_t=1.16e7)
     d.E = 7e8
     d.gamma_n = 0.0

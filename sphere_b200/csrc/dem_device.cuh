@@ -600,21 +600,46 @@ __device__ __forceinline__ void contact_writeback(const DevParams &P, const DevS
     if (P.nw > 4) S.walls_force_pp[o + 4 * np] = c.wf4;
 }
 
+// Neighbour list of sorted particle k (defined below).
+__device__ __forceinline__ void nl_build_particle(const DevParams &P, const DevState &S, unsigned k);
+
 // 6 resident blocks of 128 threads per SM (80 registers): measured best
 // between 1 and 8 on the dense-shear workload.
 #ifndef SPHB_CONTACT_MINB
 #define SPHB_CONTACT_MINB 6
 #endif
+// Contact search and forces of the per-stage path.  When the lists are
+// stale (DevCtl::nl_rebuild, raised by the integration or a re-sort) each
+// thread first rebuilds its own particle's neighbour list: only that thread
+// reads the list, so the rebuild needs no separate launch.  Every block
+// reads the flag before the last block to finish clears it.
 template <int PREC, int MODEL>
 __global__ void __launch_bounds__(128, SPHB_CONTACT_MINB) k_contacts(DevParams P, DevState S)
 {
     extern __shared__ uint32_t srow[];
+    __shared__ bool last;
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k == 0 && S.ctl->nl_rebuild) S.ctl->nl_rebuild = 0;  // k_nl_build has run
-    if (S.ctl->err || k >= P.np) return;
-    ContactOut c;
-    if (!contact_particle<PREC, MODEL>(P, S, k, srow, blockDim.x, threadIdx.x, c)) return;
-    contact_writeback(P, S, k, c);
+    DevCtl *ctl = S.ctl;
+    const bool nl = *(volatile int *)&ctl->nl_rebuild != 0;
+    if (!ctl->err && k < P.np) {
+        if (nl) nl_build_particle(P, S, k);
+        ContactOut c;
+        if (contact_particle<PREC, MODEL>(P, S, k, srow, blockDim.x, threadIdx.x, c))
+            contact_writeback(P, S, k, c);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        if (nl) {
+            ctl->nl_rebuild = 0;
+            ctl->nl_builds += 1;
+        }
+        ctl->ticket = 0;
+    }
 }
 
 // Neighbour list of sorted particle k: every candidate closer than

@@ -9,22 +9,6 @@
 
 namespace sphb {
 
-// Neighbour list build: runs every step, works only when DevCtl::nl_rebuild.
-// Also refreshes the FP32 velocity copies of the mixed mode (the rebuild
-// follows every re-sort and every write of the state from the host).
-__global__ void __launch_bounds__(128) k_nl_build(DevParams P, DevState S)
-{
-    unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (S.ctl->err || !S.ctl->nl_rebuild || k >= P.np) return;
-    nl_build_particle(P, S, k);
-    if (S.vel_f) {
-        double4 v = S.vel[k], w = S.angvel[k];
-        S.vel_f[k] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
-        S.angvel_f[k] = make_float4((float)w.x, (float)w.y, (float)w.z, 0.0f);
-    }
-    if (k == 0) S.ctl->nl_builds += 1;
-}
-
 // Occupancy masks of the slot rows (after the rows were set from the host).
 __global__ void k_occ_from_rows(DevParams P, DevState S)
 {
@@ -192,17 +176,49 @@ __global__ void __launch_bounds__(256) k_tau_partials(DevParams P, DevState S)
 // then the cell hash of the new position (src/sorting.cuh:7-51) so the
 // next step knows whether the sort changes.
 // ---------------------------------------------------------------------
+// integrate (src/integration.cuh:14-305) of the 256 sorted particles of
+// this block, then the wall reduction and wall update
+// (integration.cuh:309-450): block j forms the reference's partial sum j
+// (256 consecutive ORIGINAL indices, same tree), the block that finishes
+// last adds the partials in block order, moves the walls and advances the
+// loop counters (device.cu:2543-2545).  Launched with the reference's
+// ceil(np / 256) blocks (one block when np == 0).
 __global__ void __launch_bounds__(256) k_integrate(DevParams P, DevState S)
 {
-    unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (S.ctl->err || k >= P.np) return;
+    __shared__ double cache[256];
+    __shared__ bool last;
+    DevCtl *ctl = S.ctl;
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = ctl->err == 0;
     StepClock clk;
-    clk.iter = S.ctl->iter;
-    clk.t_current = S.ctl->t_current;
-    clk.velocity_state = S.ctl->velocity_state;
-    clk.tau_eff_x = S.ctl->tau_eff_x;
-    integrate_particle(P, S, k, S.force[k], S.torque[k], clk, S.x, S.vel, S.angvel, S.vel_f,
-                       S.angvel_f, &S.ctl->resort, &S.ctl->nl_rebuild);
+    clk.iter = ctl->iter;
+    clk.t_current = ctl->t_current;
+    clk.velocity_state = ctl->velocity_state;
+    clk.tau_eff_x = ctl->tau_eff_x;
+    if (ok && k < P.np)
+        integrate_particle(P, S, k, S.force[k], S.torque[k], clk, S.x, S.vel, S.angvel, S.vel_f,
+                           S.angvel_f, &ctl->resort, &ctl->nl_rebuild);
+    if (P.nw > 0 && P.np > 0) {
+        double s = chunk_tree_sum(S.walls_force_pp, P.np, blockIdx.x, cache);
+        if (threadIdx.x == 0) S.partials[blockIdx.x] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // every wall sums the same (wall-0) partials, as the reference does
+    double wforce = (P.nw > 0 && P.np > 0) ? ordered_sum<256>(S.partials, P.nblocks256, cache) : 0.0;
+    if (threadIdx.x != 0) return;
+    ctl->ticket = 0;
+    if (!ok || *(volatile int *)&ctl->err) return;
+    walls_integrate(P, S, wforce, clk.iter, clk.t_current);
+    ctl->velocity_state = next_velocity_state(clk.velocity_state, clk.t_current);
+    ctl->t_current = clk.t_current + P.dt;
+    ctl->iter = clk.iter + 1;
 }
 
 // Cell hash of the current positions (first step, after sph_set).
@@ -219,61 +235,15 @@ __global__ void k_hash(DevParams P, DevState S)
     S.cell_new[k] = ((unsigned)iz * P.num[1]) * P.num[0] + (unsigned)iy * P.num[0] + (unsigned)ix;
 }
 
-// Wall-force partial sums + integrateWalls (integration.cuh:344-450) in
-// the block that finishes last, then the loop counters
-// (device.cu:2543-2545).  With nw == 0 it runs as one block and only
-// advances the counters.
-__global__ void __launch_bounds__(256) k_walls_and_clock(DevParams P, DevState S)
-{
-    __shared__ double cache[256];
-    __shared__ double stage[2048];
-    __shared__ bool last;
-    DevCtl *ctl = S.ctl;
-    if (ctl->err) return;
-    if (P.nw > 0) {
-        double s = block_tree_sum(S.walls_force_pp, P.np, P.nblocks256, cache);
-        if (threadIdx.x == 0) {
-            S.partials[blockIdx.x] = s;
-            __threadfence();
-            last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
-        }
-        __syncthreads();
-    } else {
-        if (threadIdx.x == 0) last = true;
-        __syncthreads();
-    }
-    if (!last) return;
-    __threadfence();
-    // every wall sums the same (wall-0) partials, as the reference does
-    double wforce = P.nw > 0 ? ordered_sum(S.partials, P.nblocks256, stage) : 0.0;
-    if (threadIdx.x != 0) return;
-    const long long iter = ctl->iter;
-    const double t_current = ctl->t_current;
-    walls_integrate(P, S, wforce, iter, t_current);
-    ctl->velocity_state = next_velocity_state(ctl->velocity_state, t_current);
-    ctl->t_current = t_current + P.dt;
-    ctl->iter = iter + 1;
-    ctl->ticket = 0;
-}
-
 // ---------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------
 static inline unsigned blocks_for(unsigned n, unsigned b) { return (n + b - 1) / b; }
 
-cudaError_t launch_nl_build(const DevParams &P, const DevState &S, cudaStream_t st)
-{
-    if (P.np == 0) return cudaSuccess;
-    k_nl_build<<<blocks_for(P.np, 128), 128, 0, st>>>(P, S);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cudaStream_t st)
 {
     if (P.np == 0) return cudaSuccess;
     const unsigned B = 128;
-    cudaError_t e = launch_nl_build(P, S, st);
-    if (e != cudaSuccess) return e;
     dim3 grid(blocks_for(P.np, B));
     if (P.contactmodel == 2) {
         size_t smem = (size_t)B * P.nc * sizeof(uint32_t);
@@ -310,10 +280,8 @@ cudaError_t launch_integrate(const DevParams &P, const DevState &S, cudaStream_t
             k_shear_stress<<<blocks_for(P.np, 256), 256, 0, st>>>(P, S);
             k_tau_partials<<<P.nblocks256, 256, 0, st>>>(P, S);
         }
-        k_integrate<<<blocks_for(P.np, 256), 256, 0, st>>>(P, S);
     }
-    unsigned g = (P.nw > 0 && P.np > 0) ? P.nblocks256 : 1;
-    k_walls_and_clock<<<g, 256, 0, st>>>(P, S);
+    k_integrate<<<P.np > 0 ? P.nblocks256 : 1, 256, 0, st>>>(P, S);
     return cudaGetLastError();
 }
 

@@ -248,6 +248,7 @@ int Engine::allocate_and_upload()
     // initial sort (the reference sorts at the start of every step)
     if ((e = launch_hash(P, S, stream)) != cudaSuccess) return cuda_fail(e, "hash");
     if ((e = launch_resort(P, S, S.perm_scratch, 1, stream)) != cudaSuccess) return cuda_fail(e, "sort");
+    if ((e = launch_refresh_f(P, S, stream)) != cudaSuccess) return cuda_fail(e, "sort");
     return poll_errors("initial sort");
 }
 
@@ -351,7 +352,14 @@ int Engine::profile(uint64_t n, sph_profile *out)
 
 int Engine::ensure_graph()
 {
+    // kernels capture the state view by value: a graph made for the other
+    // view (the persistent path flips views) is stale
+    if (graph_exec && graph_view != cur_view) {
+        cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
     if (graph_exec || graph_steps <= 1 || graph_failed) return ST_OK;
+    graph_view = cur_view;
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { graph_failed = true; cudaGetLastError(); return ST_OK; }
@@ -372,7 +380,14 @@ int Engine::ensure_graph()
 int Engine::step(uint64_t n)
 {
     if (n == 0) return ST_OK;
-    if (persist) return step_persistent(n);
+    if (persist && !persist_off) return step_persistent(n);
+    return step_stages(n);
+}
+
+// The per-stage kernels, replayed from a CUDA graph of graph_steps steps.
+int Engine::step_stages(uint64_t n)
+{
+    if (n == 0) return ST_OK;
     if (!warmed) {
         // one eager step first: sets kernel attributes outside any capture
         cudaError_t e = enqueue_step();
@@ -951,6 +966,7 @@ int sph_get_info(sph_engine *e, sph_info *info)
     info->file_dt = g.hs.file_dt;
     info->step_count = g.hs.step_count;
     info->resorts = g.last_ctl.resorts;
+    g.persist_describe(info);
     return rc;
 }
 

@@ -55,6 +55,7 @@ public:
     DevCtl last_ctl{};
 
     cudaGraphExec_t graph_exec = nullptr;
+    int graph_view = -1;          // state view the graph was captured with
     bool graph_failed = false;
     bool warmed = false;
 
@@ -65,6 +66,7 @@ public:
     PersistDev *persist = nullptr;
     DevState S_view[2]{};         // S_view[v]: buffer view v (S is the current one)
     int cur_view = 0;
+    bool persist_off = false;     // the autotuner found the per-stage kernels faster
     FILE *convlog = nullptr;
     int jacobi_grid = 0;            // blocks of the cooperative Jacobi launch
     int darcy_exact_stop = 0;       // 1: stop at the first converged iteration
@@ -84,6 +86,7 @@ public:
     int profile(uint64_t n, struct sph_profile *out);
     int ensure_graph();
     int step(uint64_t n);
+    int step_stages(uint64_t n);
     void advance_host_clock(uint64_t n);
     int64_t field_bytes(int f) const;
     double4 *sorted_vec(int f) const;
@@ -122,6 +125,7 @@ public:
     int step_persistent(uint64_t n);
     int persist_after(uint64_t n);
     void *persist_ctl() const;    // the box's PersistCtl on the device
+    void persist_describe(struct sph_info *info) const;
 };
 
 // Opens one engine from a .bin path (path != null) or from its bytes.

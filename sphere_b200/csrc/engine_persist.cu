@@ -100,6 +100,14 @@ int Engine::persist_init()
 
 void *Engine::persist_ctl() const { return persist ? (void *)persist->pc : nullptr; }
 
+void Engine::persist_describe(sph_info *info) const
+{
+    info->step_path = (persist && !persist_off) ? 1 : 0;
+    info->step_threads = persist ? kPersistShapes[persist->shape].threads : 0;
+    info->step_grid = persist ? (int32_t)persist->grid : 0;
+    info->tuned = persist ? (persist->tuned ? 1 : 0) : 0;
+}
+
 void Engine::persist_free()
 {
     delete persist;
@@ -136,49 +144,57 @@ cudaError_t Engine::persist_launch(uint64_t n, int shape, unsigned grid)
 }
 
 // Runs n steps on the persistent path.  The first call with enough steps
-// times each block shape on real steps and keeps the fastest.
+// times each block shape -- and, unless the persistent path was requested
+// explicitly, the per-stage kernels -- on real steps and keeps the fastest.
 int Engine::step_persistent(uint64_t n)
 {
     PersistDev &D = *persist;
     uint64_t done = 0;
     const uint64_t trial = 8;
-    if (!D.tuned && n >= trial * (kNumPersistShapes + 1)) {
+    const int ncand = kNumPersistShapes + (step_kernel == 2 ? 0 : 1);
+    if (!D.tuned && n >= trial * (uint64_t)(ncand + 2)) {
         cudaEvent_t a, b;
         cudaEventCreate(&a);
         cudaEventCreate(&b);
         float best = 1e30f;
-        int best_shape = D.shape;
-        for (int sh = 0; sh < kNumPersistShapes; ++sh) {
-            unsigned g = persist_grid(sh);
+        int best_cand = D.shape;
+        int rc = ST_OK;
+        for (int cand = 0; cand < ncand && rc == ST_OK; ++cand) {
+            const bool stages = cand == kNumPersistShapes;
+            unsigned g = stages ? 1 : persist_grid(cand);
             if (!g) continue;
-            cudaEventRecord(a, stream);
-            cudaError_t e = persist_launch(trial, sh, g);
-            cudaEventRecord(b, stream);
-            if (e != cudaSuccess) {
-                cudaEventDestroy(a);
-                cudaEventDestroy(b);
-                return cuda_fail(e, "persistent step");
+            if (stages) {
+                // warm the per-stage path (eager first step, graph capture)
+                rc = step_stages(trial);
+                done += trial;
+                if (rc) break;
             }
+            cudaEventRecord(a, stream);
+            cudaError_t e = stages ? cudaSuccess : persist_launch(trial, cand, g);
+            if (stages) rc = step_stages(trial);
+            cudaEventRecord(b, stream);
+            if (e != cudaSuccess) rc = cuda_fail(e, "persistent step");
+            if (rc) break;
             cudaEventSynchronize(b);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, a, b);
             done += trial;
-            int rc = persist_after(trial);
-            if (rc) {
-                cudaEventDestroy(a);
-                cudaEventDestroy(b);
-                return rc;
-            }
+            if (!stages && (rc = persist_after(trial))) break;
             if (ms < best) {
                 best = ms;
-                best_shape = sh;
+                best_cand = cand;
             }
         }
         cudaEventDestroy(a);
         cudaEventDestroy(b);
-        D.shape = best_shape;
-        D.grid = persist_grid(best_shape);
+        if (rc) return rc;
         D.tuned = true;
+        if (best_cand == kNumPersistShapes) {
+            persist_off = true;
+            return step_stages(n - done);
+        }
+        D.shape = best_cand;
+        D.grid = persist_grid(best_cand);
     }
     if (done < n) {
         cudaError_t e = persist_launch(n - done, D.shape, D.grid);

@@ -31,13 +31,14 @@ __device__ __forceinline__ double chunk_tree_sum(const double *in, unsigned np, 
 
 // Adds in[0..n) in index order (the reference's serial loop over block
 // partials, integration.cuh:67-68, 376-378).  All threads of the calling
-// block stage chunks of 2048 in shared memory; thread 0 adds them one by
-// one.  The result is valid in thread 0.
+// block stage chunks of CHUNK values in shared memory (stage holds CHUNK
+// doubles); thread 0 adds them one by one.  The result is valid in thread 0.
+template <unsigned CHUNK = 2048>
 __device__ __forceinline__ double ordered_sum(const double *in, unsigned n, double *stage)
 {
     double acc = 0.0;
-    for (unsigned base = 0; base < n; base += 2048) {
-        unsigned m = min(2048u, n - base);
+    for (unsigned base = 0; base < n; base += CHUNK) {
+        unsigned m = min(CHUNK, n - base);
         __syncthreads();
         for (unsigned i = threadIdx.x; i < m; i += blockDim.x) stage[i] = __ldcg(in + base + i);
         __syncthreads();

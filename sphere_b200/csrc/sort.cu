@@ -59,7 +59,8 @@ __global__ void __launch_bounds__(256) k_resort(DevParams P, DevState S, PermScr
     if (ctl->err) return;
     if (!force && !ctl->resort) return;
     auto bar = [&]() { return grid_barrier(ctl, gridDim.x); };
-    if (!resort_group(P, S, W, gridDim.x, blockIdx.x, bar, false)) return;
+    // the FP32 velocity copies of the mixed mode follow the permutation
+    if (!resort_group(P, S, W, gridDim.x, blockIdx.x, bar, true)) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctl->resort = 0;
         ctl->resorts += 1;

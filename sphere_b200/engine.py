@@ -56,7 +56,9 @@ class SphInfo(ctypes.Structure):
                 ("iter", ctypes.c_int64), ("time", ctypes.c_double),
                 ("time_total", ctypes.c_double), ("dt", ctypes.c_double),
                 ("file_dt", ctypes.c_double), ("step_count", ctypes.c_uint32),
-                ("resorts", ctypes.c_int64)]
+                ("resorts", ctypes.c_int64), ("step_path", ctypes.c_int32),
+                ("step_threads", ctypes.c_int32), ("step_grid", ctypes.c_int32),
+                ("tuned", ctypes.c_int32)]
 
 
 class SphProfile(ctypes.Structure):
