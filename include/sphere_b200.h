@@ -268,21 +268,22 @@ const char *sph_batch_last_error(sph_batch *b);
 void sph_batch_close(sph_batch *b);
 
 /* ---------------------------------------------------------------------
- * The warm-start network alone (3 -> 16 -> 16 -> 1 channels, 3x3x3
+ * The warm-start network alone (4 -> 16 -> 16 -> 1 channels, 3x3x3
  * kernels, ReLU; BF16 tensor-core kernels with FP32 accumulation) on host
  * arrays, for gradient checks.  The engine uses it through
  * sph_opts.warm_start.  Layer parameters: w [27 taps][16 out][16 in]
- * (taps z-major, then y, then x, offsets -1..1), b [16].  Inputs: 3
- * normalised channels per cell (x fastest); output: channel 0 of layer 3.
+ * (taps z-major, then y, then x, offsets -1..1), b [16].  Inputs: 4
+ * normalised channels per cell (x fastest: previous pressure, porosity,
+ * porosity change, previous pressure change); output: channel 0 of layer 3.
  * --------------------------------------------------------------------- */
 typedef struct sph_wsnet sph_wsnet;
 int sph_wsnet_create(int nx, int ny, int nz, uint64_t seed, sph_wsnet **out);
 int sph_wsnet_set_params(sph_wsnet *n, int layer, const float *w, const float *b);
 int sph_wsnet_get_params(sph_wsnet *n, int layer, float *w, float *b);
-int sph_wsnet_forward(sph_wsnet *n, const float *x3, float *out);
+int sph_wsnet_forward(sph_wsnet *n, const float *x4, float *out);
 /* Gradients of the mean squared error over free cells (free_cells[c] != 0)
  * between the output and target: dw = 3 x [27][16][16], db = 3 x [16]. */
-int sph_wsnet_gradients(sph_wsnet *n, const float *x3, const float *target,
+int sph_wsnet_gradients(sph_wsnet *n, const float *x4, const float *target,
                         const unsigned char *free_cells, float *dw, float *db);
 void sph_wsnet_destroy(sph_wsnet *n);
 

@@ -1,7 +1,7 @@
 """CPU oracle of the Darcy warm-start network -- TEST INFRASTRUCTURE ONLY.
 
 A plain numpy restatement of the network the engine trains on the tensor
-cores (3 -> 16 -> 16 -> 1 channels, 3x3x3 kernels with zero padding, ReLU
+cores (4 -> 16 -> 16 -> 1 channels, 3x3x3 kernels with zero padding, ReLU
 after layers 1 and 2), its mean-squared-error loss over free cells and the
 gradients of every weight and bias.  Arithmetic is float64; with
 ``bf16=True`` the values are rounded to BF16 (round to nearest even) at the
@@ -10,13 +10,14 @@ activations after ReLU, and the gradients stored between layers.  Without
 rounding the gradients are exact and are checked against finite
 differences in tests/test_warmstart_oracle.py.
 
-Layouts match the C ABI: inputs [ncells][3] and outputs [ncells] with x
+Layouts match the C ABI: inputs [ncells][4] and outputs [ncells] with x
 fastest; weights [27 taps][16 out][16 in] with tap = (dz+1)*9 + (dy+1)*3 +
 (dx+1); biases [16].
 """
 import numpy as np
 
 TAPS = [(dz, dy, dx) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)]
+INPUTS = 4   # previous pressure, porosity, porosity change, previous pressure change
 
 
 def bf16_round(a):
@@ -76,9 +77,9 @@ class Net:
     def _grid(self, a):
         return a.reshape(self.nz, self.ny, self.nx, -1)
 
-    def forward(self, x3):
+    def forward(self, x4):
         x0 = np.zeros((self.nz, self.ny, self.nx, 16))
-        x0[..., :3] = self._grid(self.r(np.asarray(x3, dtype=np.float64)))
+        x0[..., :INPUTS] = self._grid(self.r(np.asarray(x4, dtype=np.float64)))
         a1 = self.r(np.maximum(conv(x0, self.w[0]) + self.b[0], 0.0))
         a2 = self.r(np.maximum(conv(a1, self.w[1]) + self.b[1], 0.0))
         out = conv(a2, self.w[2])[..., 0] + self.b[2][0]
@@ -107,12 +108,12 @@ class Net:
 
 
 def random_params(seed, scale=1.0):
-    """Parameters with the engine's structure: layer 1 reads 3 channels,
-    layer 3 writes channel 0 only."""
+    """Parameters with the engine's structure: layer 1 reads INPUTS
+    channels, layer 3 writes channel 0 only."""
     rng = np.random.default_rng(seed)
     out = []
     for layer in range(3):
-        cin = 3 if layer == 0 else 16
+        cin = INPUTS if layer == 0 else 16
         cout = 1 if layer == 2 else 16
         w = np.zeros((27, 16, 16), dtype=np.float32)
         w[:, :cout, :cin] = rng.normal(0.0, scale * np.sqrt(2.0 / (27 * cin)), (27, cout, cin))

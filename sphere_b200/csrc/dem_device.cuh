@@ -386,15 +386,23 @@ struct ContactOut {
 };
 
 // Contact search + forces of sorted particle k (topology and interact of
-// the reference, walls included).  srow is the thread's slot-row scratch in
-// shared memory (entry i at srow[i * B + t]).  Returns false after raising
-// a capacity error.
+// the reference, walls included).  srow / skb are the thread's slot scratch
+// in shared memory (entry i at [i * B + t]): the partner's original index
+// and, for partners found overlapping this step, its sorted index.
+// Returns false after raising a capacity error.
 // PREC 0: faithful FP64, 1: FP64, 2: mixed (FP64 overlap, FP32 contact law,
 // FP64 accumulation).
+//
+// Every overlapping pair is in the neighbour list and the topology visit
+// computes exactly the overlap the reference's interact recomputes (same
+// operands, same operation order), so a slot is in contact this step iff
+// topology hit it: interact evaluates the hit slots in slot order with the
+// partner's sorted index at hand, and clears the other occupied slots
+// without loading their partners.
 template <int PREC, int MODEL>
 __device__ __forceinline__ bool contact_particle(const DevParams &P, const DevState &S, unsigned k,
-                                                 uint32_t *srow, unsigned B, unsigned t,
-                                                 ContactOut &out)
+                                                 uint32_t *srow, uint32_t *skb, unsigned B,
+                                                 unsigned t, ContactOut &out)
 {
     constexpr int TP = PREC == 2 ? 1 : PREC;  // precision of overlap tests
     const unsigned NC = P.nc;
@@ -412,7 +420,7 @@ __device__ __forceinline__ bool contact_particle(const DevParams &P, const DevSt
     if (MODEL == 2) {
         const size_t rowbase = (size_t)o * NC;
         uint64_t mask = S.occ[o];
-        uint64_t written = 0;
+        uint64_t written = 0, hit = 0;
         {
             uint64_t m = mask;
             while (m) {
@@ -440,8 +448,10 @@ __device__ __forceinline__ bool contact_particle(const DevParams &P, const DevSt
                     return false;
                 }
                 srow[cpos * B + t] = b_orig;
+                skb[cpos * B + t] = b;
                 mask |= 1ull << cpos;
                 written |= 1ull << cpos;
+                hit |= 1ull << cpos;
                 S.dmcode[rowbase + cpos] = dm_encode(sx, sy);
                 ++nc;
             }
@@ -459,38 +469,42 @@ __device__ __forceinline__ bool contact_particle(const DevParams &P, const DevSt
             for_each_cell_candidate(P, S, k, xa, visit);
         }
         if (!ok) return false;
-        // --- interact, history contacts in slot order ---
-        uint64_t m = mask;
+        // --- interact: occupied slots that were not hit are no longer in
+        // contact; the hit slots get forces in slot order ---
+        {
+            uint64_t gone = mask & ~hit;
+            while (gone) {
+                const int i = __ffsll((long long)gone) - 1;
+                gone &= gone - 1;
+                const size_t mempos = rowbase + i;
+                mask &= ~(1ull << i);
+                written |= 1ull << i;
+                if constexpr (PREC == 2) S.delta_t_f[mempos] = make_float4(0.f, 0.f, 0.f, 0.f);
+                else S.delta_t[mempos] = make_double4(0.0, 0.0, 0.0, 0.0);
+            }
+        }
+        uint64_t m = hit;
         while (m) {
             const int i = __ffsll((long long)m) - 1;
             m &= m - 1;
-            const unsigned b_orig = srow[i * B + t];
-            if (b_orig >= P.np) { raise_err(S.ctl, DERR_CAPACITY, (int)o); return false; }
             const size_t mempos = rowbase + i;
+            const unsigned kb = skb[i * B + t];
             V3 dm = dm_decode(P, S.dmcode[mempos]);
-            unsigned kb = S.pos_of[b_orig];
             double4 xb = S.x[kb];
             double rb = xb.w;
             V3 x_ab = mk3(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
             double len = vlen<TP>(x_ab);
             double delta_n = len - (ra + rb);
-            if (delta_n < 0.0) {
-                if constexpr (PREC == 2) {
-                    float4 h = S.delta_t_f[mempos];
-                    mixed_pair(P, F, T, es_dot, ev_dot, p, S.vel_f[k], S.angvel_f[k], S.vel_f[kb],
-                               S.angvel_f[kb], h, ra, rb, x_ab, len, delta_n);
-                    S.delta_t_f[mempos] = h;
-                } else {
-                    V3 dt_new = contact_linear<PREC>(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a,
-                                                     S.vel[kb], xyz(S.angvel[kb]),
-                                                     S.delta_t[mempos], ra, rb, x_ab, len, delta_n);
-                    S.delta_t[mempos] = make_double4(dt_new.x, dt_new.y, dt_new.z, 0.0);
-                }
+            if constexpr (PREC == 2) {
+                float4 h = S.delta_t_f[mempos];
+                mixed_pair(P, F, T, es_dot, ev_dot, p, S.vel_f[k], S.angvel_f[k], S.vel_f[kb],
+                           S.angvel_f[kb], h, ra, rb, x_ab, len, delta_n);
+                S.delta_t_f[mempos] = h;
             } else {
-                mask &= ~(1ull << i);
-                written |= 1ull << i;
-                if constexpr (PREC == 2) S.delta_t_f[mempos] = make_float4(0.f, 0.f, 0.f, 0.f);
-                else S.delta_t[mempos] = make_double4(0.0, 0.0, 0.0, 0.0);
+                V3 dt_new = contact_linear<PREC>(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a,
+                                                 S.vel[kb], xyz(S.angvel[kb]), S.delta_t[mempos],
+                                                 ra, rb, x_ab, len, delta_n);
+                S.delta_t[mempos] = make_double4(dt_new.x, dt_new.y, dt_new.z, 0.0);
             }
         }
         if (written) {
@@ -608,38 +622,19 @@ __device__ __forceinline__ void nl_build_particle(const DevParams &P, const DevS
 #ifndef SPHB_CONTACT_MINB
 #define SPHB_CONTACT_MINB 6
 #endif
-// Contact search and forces of the per-stage path.  When the lists are
-// stale (DevCtl::nl_rebuild, raised by the integration or a re-sort) each
-// thread first rebuilds its own particle's neighbour list: only that thread
-// reads the list, so the rebuild needs no separate launch.  Every block
-// reads the flag before the last block to finish clears it.
+// Contact search and forces of the per-stage path (after k_nl_build).
 template <int PREC, int MODEL>
 __global__ void __launch_bounds__(128, SPHB_CONTACT_MINB) k_contacts(DevParams P, DevState S)
 {
-    extern __shared__ uint32_t srow[];
-    __shared__ bool last;
+    extern __shared__ uint32_t srow[];   // blockDim * nc slot partners, then as many sorted indices
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    DevCtl *ctl = S.ctl;
-    const bool nl = *(volatile int *)&ctl->nl_rebuild != 0;
-    if (!ctl->err && k < P.np) {
-        if (nl) nl_build_particle(P, S, k);
-        ContactOut c;
-        if (contact_particle<PREC, MODEL>(P, S, k, srow, blockDim.x, threadIdx.x, c))
-            contact_writeback(P, S, k, c);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        if (nl) {
-            ctl->nl_rebuild = 0;
-            ctl->nl_builds += 1;
-        }
-        ctl->ticket = 0;
-    }
+    if (k == 0 && S.ctl->nl_rebuild) S.ctl->nl_rebuild = 0;  // k_nl_build has run
+    if (S.ctl->err || k >= P.np) return;
+    ContactOut c;
+    if (!contact_particle<PREC, MODEL>(P, S, k, srow, srow + (size_t)blockDim.x * P.nc, blockDim.x,
+                                       threadIdx.x, c))
+        return;
+    contact_writeback(P, S, k, c);
 }
 
 // Neighbour list of sorted particle k: every candidate closer than

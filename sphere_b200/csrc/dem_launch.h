@@ -12,6 +12,8 @@ namespace sphb {
 cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cudaStream_t st);
 // mixed precision: FP64 overlaps, FP32 contact laws, FP64 accumulation
 cudaError_t launch_contacts_mixed(const DevParams &P, const DevState &S, cudaStream_t st);
+// neighbour-list rebuild (a no-op unless DevCtl::nl_rebuild)
+cudaError_t launch_nl_build(const DevParams &P, const DevState &S, cudaStream_t st);
 cudaError_t launch_bonds(const DevParams &P, const DevState &S, int prec, double4 *bond_f,
                          double4 *bond_t, cudaStream_t st);
 // shear-stress reduction (wmode 3), then one kernel: integration, wall

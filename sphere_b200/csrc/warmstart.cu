@@ -1,7 +1,8 @@
 // Learned warm start for the Darcy pressure solve: a 3-layer 3D convolution
-// network (3 -> 16 -> 16 -> 1 channels, 3x3x3 kernels, ReLU) maps the
-// previous pressure, the porosity and the porosity change of a fluid step
-// to the pressure change of the step's solve.  It is trained online on the
+// network (4 -> 16 -> 16 -> 1 channels, 3x3x3 kernels, ReLU) maps the
+// previous pressure, the porosity, the porosity change of a fluid step and
+// the previous solve's pressure change to the pressure change of the step's
+// solve.  It is trained online on the
 // solves the engine itself makes: after each solve the converged pressure
 // is the target, one Adam step follows.
 //
@@ -31,6 +32,7 @@ namespace sphb {
 namespace {
 
 constexpr int kCh = 16;          // channels of every activation (inputs padded)
+constexpr int kInputs = 4;       // p_prev, phi, dphi, previous pressure change
 constexpr int kTaps = 27;
 constexpr int kWElems = kTaps * kCh * kCh;   // weights per layer
 constexpr int kTile = 128;       // cells per MMA tile (M)
@@ -312,8 +314,18 @@ struct Scalars {
     float dp_scale;
     int dp_init;
     float loss;
-    int pad;
+    float wsum;      // sum of the loss weights over free cells
 };
+
+// Loss weight of a cell: the solve stops on the largest RELATIVE change
+// |dp| / |p| (darcy.cuh, device.cu:2340-2366), so cells with small |p|
+// decide the iteration count; the loss weighs errors by 1 / (|p| / pmax +
+// 1e-3)^2 to match.
+__device__ __forceinline__ float loss_weight(double p, float pscale)
+{
+    const float r = fabsf((float)p) / pscale + 1e-3f;
+    return 1.0f / (r * r);
+}
 
 __device__ __forceinline__ unsigned didx_ws(int nx, int ny, int x, int y, int z)
 {
@@ -348,7 +360,7 @@ __global__ void k_stats(int nx, int ny, int nz, const double *p, const double *d
 }
 
 __global__ void k_features(int nx, int ny, int nz, const double *p, const double *phi,
-                           const double *dphi, const Scalars *sc, bf16 *x0)
+                           const double *dphi, const float *dp_last, const Scalars *sc, bf16 *x0)
 {
     const unsigned n = (unsigned)nx * ny * nz;
     const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -357,13 +369,14 @@ __global__ void k_features(int nx, int ny, int nz, const double *p, const double
     const unsigned g = didx_ws(nx, ny, x, y, z);
     const float ps = fmaxf(__uint_as_float(sc->pmax_bits), 1.0f);
     const float ds = __uint_as_float(sc->dphimax_bits);
-    float f[3];
+    float f[4];
     f[0] = (float)p[g] / ps;
     f[1] = ((float)phi[g] - 0.5f) * 2.0f;
     f[2] = ds > 0.0f ? (float)dphi[g] / ds : 0.0f;
+    f[3] = sc->dp_init ? dp_last[c] / sc->dp_scale : 0.0f;
     __align__(16) __nv_bfloat162 pk[8];
     pk[0] = __floats2bfloat162_rn(f[0], f[1]);
-    pk[1] = __floats2bfloat162_rn(f[2], 0.0f);
+    pk[1] = __floats2bfloat162_rn(f[2], f[3]);
     for (int j = 2; j < 8; ++j) pk[j] = __floats2bfloat162_rn(0.0f, 0.0f);
     uint4 *dst = reinterpret_cast<uint4 *>(x0 + (size_t)c * 16);
     dst[0] = *reinterpret_cast<const uint4 *>(&pk[0]);
@@ -384,16 +397,21 @@ __global__ void k_compose(int nx, int ny, int nz, const double *p, const float *
     guess[g] = v;
 }
 
+// the pressure change of the solve just made: its maximum over free cells
+// (for the running scale) and the change itself (an input of the next
+// prediction)
 __global__ void k_dpmax(int nx, int ny, int nz, const double *p_prev, const double *p_star,
-                        const unsigned char *freec, Scalars *sc)
+                        const unsigned char *freec, Scalars *sc, float *dp_last)
 {
     const unsigned n = (unsigned)nx * ny * nz;
     const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
     float m = 0.0f;
-    if (c < n && freec[c]) {
+    if (c < n) {
         const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((unsigned)nx * ny));
         const unsigned g = didx_ws(nx, ny, x, y, z);
-        m = fabsf((float)(p_star[g] - p_prev[g]));
+        const float d = (float)(p_star[g] - p_prev[g]);
+        dp_last[c] = freec[c] ? d : 0.0f;
+        if (freec[c]) m = fabsf(d);
     }
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) atomicMax(&sc->dpmax_bits, __float_as_uint(m));
@@ -412,7 +430,37 @@ __global__ void k_dpscale(Scalars *sc)
     }
 }
 
-// gradient of the mean squared error over free cells at the output
+// per-block sums of the loss weights over free cells (tree in block order)
+__global__ void k_weight_partials(int nx, int ny, int nz, const double *p_prev,
+                                  const unsigned char *freec, const Scalars *sc, float *partial)
+{
+    __shared__ float red[256];
+    const unsigned n = (unsigned)nx * ny * nz;
+    const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
+    float w = 0.0f;
+    if (c < n && freec[c]) {
+        const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((unsigned)nx * ny));
+        w = loss_weight(p_prev[didx_ws(nx, ny, x, y, z)], fmaxf(__uint_as_float(sc->pmax_bits), 1.0f));
+    }
+    red[threadIdx.x] = w;
+    __syncthreads();
+    for (unsigned i = 128; i; i >>= 1) {
+        if (threadIdx.x < i) red[threadIdx.x] += red[threadIdx.x + i];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+__global__ void k_weight_sum(const float *partial, unsigned nb, Scalars *sc)
+{
+    float s = 0.0f;
+    for (unsigned b = 0; b < nb; ++b) s += partial[b];
+    sc->wsum = s;
+}
+
+// gradient of the loss over free cells at the output: the weighted mean
+// squared error of the normalised pressure change, or with
+// target_override the plain mean squared error against that target
 __global__ void k_loss_grad(int nx, int ny, int nz, const double *p_prev, const double *p_star,
                             const float *out, const unsigned char *freec, Scalars *sc, bf16 *g3,
                             const float *target_override)
@@ -422,18 +470,21 @@ __global__ void k_loss_grad(int nx, int ny, int nz, const double *p_prev, const 
     if (c >= n) return;
     float grad = 0.0f;
     if (freec[c]) {
-        float t;
+        float t, w, wsum;
         if (target_override) {
             t = target_override[c];
+            w = 1.0f;
+            wsum = (float)max(sc->nfree, 1u);
         } else {
             const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((unsigned)nx * ny));
             const unsigned g = didx_ws(nx, ny, x, y, z);
             t = (float)((p_star[g] - p_prev[g]) / (double)sc->dp_scale);
+            w = loss_weight(p_prev[g], fmaxf(__uint_as_float(sc->pmax_bits), 1.0f));
+            wsum = fmaxf(sc->wsum, 1e-30f);
         }
         const float e = out[c] - t;
-        const float nf = (float)max(sc->nfree, 1u);
-        grad = 2.0f * e / nf;
-        atomicAdd(&sc->loss, e * e / nf);
+        grad = 2.0f * w * e / wsum;
+        atomicAdd(&sc->loss, w * e * e / wsum);
     }
     __align__(16) __nv_bfloat162 pk[8];
     pk[0] = __floats2bfloat162_rn(grad, 0.0f);
@@ -443,14 +494,14 @@ __global__ void k_loss_grad(int nx, int ny, int nz, const double *p_prev, const 
     dst[1] = *reinterpret_cast<const uint4 *>(&pk[4]);
 }
 
-// raw (already normalised) 3-channel inputs -> BF16 activations (test hook)
-__global__ void k_pack_inputs(const float *x3, unsigned n, bf16 *x0)
+// raw (already normalised) 4-channel inputs -> BF16 activations (test hook)
+__global__ void k_pack_inputs(const float *x4, unsigned n, bf16 *x0)
 {
     const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     __align__(16) __nv_bfloat162 pk[8];
-    pk[0] = __floats2bfloat162_rn(x3[3 * c], x3[3 * c + 1]);
-    pk[1] = __floats2bfloat162_rn(x3[3 * c + 2], 0.0f);
+    pk[0] = __floats2bfloat162_rn(x4[4 * c], x4[4 * c + 1]);
+    pk[1] = __floats2bfloat162_rn(x4[4 * c + 2], x4[4 * c + 3]);
     for (int j = 2; j < 8; ++j) pk[j] = __floats2bfloat162_rn(0.0f, 0.0f);
     uint4 *dst = reinterpret_cast<uint4 *>(x0 + (size_t)c * 16);
     dst[0] = *reinterpret_cast<const uint4 *>(&pk[0]);
@@ -472,7 +523,10 @@ struct WarmStart {
     float *partial_w = nullptr, *partial_b = nullptr;
     unsigned wgrad_blocks = 0, cells_per_block = 0;
     unsigned char *freec = nullptr;
+    float *dp_last = nullptr;       // pressure change of the last solve (free cells)
+    float *wpartial = nullptr;      // per-block loss-weight sums
     Scalars *sc = nullptr;
+    int train_iters = 2;            // Adam steps per solve while training
     int *err = nullptr;
     const double *last_p_prev = nullptr;
     int adam_t = 0;
@@ -591,6 +645,8 @@ WarmStart *ws_create(int nx, int ny, int nz, uint64_t seed, int train_solves)
     W->g3 = W->alloc<bf16>(act); W->g2 = W->alloc<bf16>(act); W->g1 = W->alloc<bf16>(act);
     W->out = W->alloc<float>(W->ncells);
     W->freec = W->alloc<unsigned char>(W->ncells);
+    W->dp_last = W->alloc<float>(W->ncells);
+    W->wpartial = W->alloc<float>(blocks(W->ncells, 256));
     W->sc = W->alloc<Scalars>(1);
     W->err = W->alloc<int>(1);
     // one weight-gradient block per ~1024 cells, at least one 128-cell tile
@@ -607,7 +663,7 @@ WarmStart *ws_create(int nx, int ny, int nz, uint64_t seed, int train_solves)
         W->dw[l] = W->alloc<float>(kWElems); W->db[l] = W->alloc<float>(16);
         W->w_bf[l] = W->alloc<bf16>(kWElems); W->wt_bf[l] = W->alloc<bf16>(kWElems);
         // He initialisation over the real fan-in; unused channels stay zero
-        const int cin = l == 0 ? 3 : 16, cout = l == 2 ? 1 : 16;
+        const int cin = l == 0 ? kInputs : 16, cout = l == 2 ? 1 : 16;
         const float stdv = l == 2 ? 1e-3f : std::sqrt(2.0f / (27.0f * cin));
         std::vector<float> h(kWElems, 0.0f);
         for (int tap = 0; tap < kTaps; ++tap)
@@ -641,7 +697,8 @@ cudaError_t ws_predict(WarmStart *W, const WSDarcyInputs &in, double *guess, cud
     if ((e = cudaMemsetAsync(W->sc, 0, 16, st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(&W->sc->loss, 0, 4, st)) != cudaSuccess) return e;
     k_stats<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, in.p, in.dphi, W->freec, W->sc);
-    k_features<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, in.p, in.phi, in.dphi, W->sc, W->x0);
+    k_features<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, in.p, in.phi, in.dphi,
+                                              W->dp_last, W->sc, W->x0);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = forward(*W, st)) != cudaSuccess) return e;
     k_compose<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, in.p, W->out, W->freec, W->sc, guess);
@@ -652,16 +709,26 @@ cudaError_t ws_predict(WarmStart *W, const WSDarcyInputs &in, double *guess, cud
 
 cudaError_t ws_train(WarmStart *W, const double *p_prev, const double *p_star, cudaStream_t st)
 {
-    if (W->trained >= W->train_budget) return cudaSuccess;
     const unsigned n = W->ncells;
     cudaError_t e;
-    k_dpmax<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, p_star, W->freec, W->sc);
+    // every solve: the running scale and the change the next prediction reads
+    k_dpmax<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, p_star, W->freec, W->sc,
+                                            W->dp_last);
     k_dpscale<<<1, 1, 0, st>>>(W->sc);
-    k_loss_grad<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, p_star, W->out,
-                                                W->freec, W->sc, W->g3, nullptr);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = backward(*W, st)) != cudaSuccess) return e;
-    if ((e = adam_step(*W, st)) != cudaSuccess) return e;
+    if (W->trained >= W->train_budget) return cudaSuccess;
+    k_weight_partials<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, W->freec, W->sc,
+                                                      W->wpartial);
+    k_weight_sum<<<1, 1, 0, st>>>(W->wpartial, blocks(n, 256), W->sc);
+    for (int it = 0; it < W->train_iters; ++it) {
+        if (it > 0 && (e = forward(*W, st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(&W->sc->loss, 0, 4, st)) != cudaSuccess) return e;
+        k_loss_grad<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, p_star, W->out,
+                                                    W->freec, W->sc, W->g3, nullptr);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = backward(*W, st)) != cudaSuccess) return e;
+        if ((e = adam_step(*W, st)) != cudaSuccess) return e;
+    }
     W->trained += 1;
     return cudaSuccess;
 }
@@ -700,12 +767,12 @@ int ws_get_params(WarmStart *W, int layer, float *w, float *b)
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1;
 }
 
-int ws_forward_host(WarmStart *W, const float *x3, float *out)
+int ws_forward_host(WarmStart *W, const float *x4, float *out)
 {
     const unsigned n = W->ncells;
     float *dx = nullptr;
-    if (cudaMalloc(&dx, (size_t)n * 12) != cudaSuccess) return -1;
-    cudaMemcpy(dx, x3, (size_t)n * 12, cudaMemcpyHostToDevice);
+    if (cudaMalloc(&dx, (size_t)n * 16) != cudaSuccess) return -1;
+    cudaMemcpy(dx, x4, (size_t)n * 16, cudaMemcpyHostToDevice);
     k_pack_inputs<<<blocks(n, 256), 256>>>(dx, n, W->x0);
     cudaError_t e = forward(*W, nullptr);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -715,12 +782,12 @@ int ws_forward_host(WarmStart *W, const float *x3, float *out)
     return ws_error(W, nullptr) ? -2 : 0;
 }
 
-int ws_gradients_host(WarmStart *W, const float *x3, const float *target, const unsigned char *freec,
+int ws_gradients_host(WarmStart *W, const float *x4, const float *target, const unsigned char *freec,
                       float *dw, float *db)
 {
     const unsigned n = W->ncells;
     std::vector<float> out(n);
-    if (ws_forward_host(W, x3, out.data())) return -1;
+    if (ws_forward_host(W, x4, out.data())) return -1;
     float *dt = nullptr;
     if (cudaMalloc(&dt, (size_t)n * 4) != cudaSuccess) return -1;
     cudaMemcpy(dt, target, (size_t)n * 4, cudaMemcpyHostToDevice);
@@ -775,16 +842,16 @@ int sph_wsnet_get_params(sph_wsnet *n, int layer, float *w, float *b)
     return (n && w && b) ? sphb::ws_get_params(n->w, layer, w, b) : -8;
 }
 
-int sph_wsnet_forward(sph_wsnet *n, const float *x3, float *out)
+int sph_wsnet_forward(sph_wsnet *n, const float *x4, float *out)
 {
-    return (n && x3 && out) ? sphb::ws_forward_host(n->w, x3, out) : -8;
+    return (n && x4 && out) ? sphb::ws_forward_host(n->w, x4, out) : -8;
 }
 
-int sph_wsnet_gradients(sph_wsnet *n, const float *x3, const float *target,
+int sph_wsnet_gradients(sph_wsnet *n, const float *x4, const float *target,
                         const unsigned char *free_cells, float *dw, float *db)
 {
-    return (n && x3 && target && free_cells && dw && db)
-               ? sphb::ws_gradients_host(n->w, x3, target, free_cells, dw, db)
+    return (n && x4 && target && free_cells && dw && db)
+               ? sphb::ws_gradients_host(n->w, x4, target, free_cells, dw, db)
                : -8;
 }
 

@@ -22,8 +22,10 @@ void ws_destroy(WarmStart *w);
 // Network prediction for this solve: guess = p + free * predicted change
 // (interior cells of the padded guess array).
 cudaError_t ws_predict(WarmStart *w, const WSDarcyInputs &in, double *guess, cudaStream_t st);
-// One Adam step towards the solve's result p_star from p_prev (the inputs
-// of the last prediction); nothing once the training budget is spent.
+// After a solve: records its pressure change (an input of the next
+// prediction) and the running scale; while the training budget lasts, Adam
+// steps towards the solve's result p_star from p_prev (the inputs of the
+// last prediction).
 cudaError_t ws_train(WarmStart *w, const double *p_prev, const double *p_star, cudaStream_t st);
 int ws_trained(const WarmStart *w);
 int ws_predictions(const WarmStart *w);
@@ -31,7 +33,7 @@ int ws_error(WarmStart *w, cudaStream_t st);
 float ws_last_loss(WarmStart *w, cudaStream_t st);
 
 // test hooks on host arrays: parameters of layer 0..2 (w: [27][16 out][16 in],
-// b: [16]), forward of already-normalised 3-channel inputs, and the
+// b: [16]), forward of already-normalised 4-channel inputs, and the
 // gradients of the mean squared error over free cells
 int ws_set_params(WarmStart *w, int layer, const float *wt, const float *b);
 int ws_get_params(WarmStart *w, int layer, float *wt, float *b);

@@ -409,16 +409,18 @@ class WSNet:
             raise EngineError(-4, "get_params failed")
         return w, b
 
-    def forward(self, x3):
-        x3 = numpy.ascontiguousarray(x3, dtype=numpy.float32)
+    def forward(self, x4):
+        x3 = numpy.ascontiguousarray(x4, dtype=numpy.float32)
+        assert x3.size == 4 * self.ncells
         out = numpy.empty(self.ncells, dtype=numpy.float32)
         rc = lib().sph_wsnet_forward(self._h, x3.ctypes.data, out.ctypes.data)
         if rc:
             raise EngineError(rc, "forward failed")
         return out
 
-    def gradients(self, x3, target, free):
-        x3 = numpy.ascontiguousarray(x3, dtype=numpy.float32)
+    def gradients(self, x4, target, free):
+        x3 = numpy.ascontiguousarray(x4, dtype=numpy.float32)
+        assert x3.size == 4 * self.ncells
         target = numpy.ascontiguousarray(target, dtype=numpy.float32)
         free = numpy.ascontiguousarray(free, dtype=numpy.uint8)
         dw = numpy.empty((3, 27, 16, 16), dtype=numpy.float32)

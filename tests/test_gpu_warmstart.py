@@ -19,7 +19,7 @@ def _case(shape, seed):
     nx, ny, nz = shape
     n = nx * ny * nz
     rng = numpy.random.default_rng(seed)
-    x3 = rng.normal(size=(n, 3)).astype(numpy.float32)
+    x3 = rng.normal(size=(n, WO.INPUTS)).astype(numpy.float32)
     target = rng.normal(size=n).astype(numpy.float32)
     free = (rng.uniform(size=n) > 0.15).astype(numpy.uint8)
     return x3, target, free
@@ -45,7 +45,7 @@ def test_network_matches_oracle(shape):
         eb = numpy.linalg.norm(db[layer] - db_ref[layer]) / max(numpy.linalg.norm(db_ref[layer]), 1e-30)
         assert eb <= 2e-2, (layer, eb)
     # structure: unused input channels and output channels get no gradient
-    assert numpy.all(dw[0][:, :, 3:] == 0.0) and numpy.all(dw[2][:, 1:, :] == 0.0)
+    assert numpy.all(dw[0][:, :, WO.INPUTS:] == 0.0) and numpy.all(dw[2][:, 1:, :] == 0.0)
     net.close()
 
 

@@ -21,7 +21,7 @@ def test_gradients_match_finite_differences():
     n = 4 * 3 * 5
     rng = np.random.default_rng(3)
     params = [(w.astype(np.float64), b.astype(np.float64)) for w, b in W.random_params(11, 2.0)]
-    x3 = rng.normal(size=(n, 3))
+    x3 = rng.normal(size=(n, W.INPUTS))
     target = rng.normal(size=n)
     free = (rng.uniform(size=n) > 0.2).astype(np.uint8)
 
@@ -36,7 +36,7 @@ def test_gradients_match_finite_differences():
     eps = 1e-6
     checked = 0
     for layer in range(3):
-        cin = 3 if layer == 0 else 16
+        cin = W.INPUTS if layer == 0 else 16
         cout = 1 if layer == 2 else 16
         for _ in range(12):
             t, o, i = rng.integers(27), rng.integers(cout), rng.integers(cin)
@@ -56,5 +56,5 @@ def test_gradients_match_finite_differences():
         assert abs(fd - db[layer][o]) <= 1e-5 * max(1.0, abs(fd))
     assert checked == 36
     # unused channels get exactly zero gradient
-    assert np.all(dw[0][:, :, 3:] == 0.0) and np.all(dw[2][:, 1:, :] == 0.0)
+    assert np.all(dw[0][:, :, W.INPUTS:] == 0.0) and np.all(dw[2][:, 1:, :] == 0.0)
     assert np.all(db[2][1:] == 0.0)
