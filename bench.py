@@ -218,7 +218,13 @@ def run_gpu(args):
     bytes_per_particle = 184.0 + 56.0 * zbar
     contacts_bytes = n * bytes_per_particle
     achieved = contacts_bytes / (prof.contacts_ms * 1e-3) / 1e9
-    launches_per_dem_step = 5 + (2 if d.nw > 0 and d.wmode[0] == 3 else 0)
+    # launches of this library's kernels in the timed region: per DEM step
+    # k_resort, k_nl_build, k_contacts, k_integrate (+2 for the shear-stress
+    # wall) on the per-stage path; one k_persistent per call on the fused path
+    if info.step_path == 1:
+        timed_launches = args.steps
+    else:
+        timed_launches = (4 + (2 if d.nw > 0 and d.wmode[0] == 3 else 0)) * INTERVAL * args.steps
     out = {
         "metric": "particle-steps/s",
         "value": value,
@@ -243,7 +249,7 @@ def run_gpu(args):
         },
         "e2e": {"value": e2e_value, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": 3 * 32 * n, "d2h_bytes_per_step": 5 * 32 * n},
-        "gpu_launches": launches_per_dem_step * INTERVAL * args.steps,
+        "gpu_launches": timed_launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None,
                      "kernel": "k_contacts (contact search + forces)",
@@ -430,6 +436,8 @@ def main():
     ap.add_argument("--batch-boxes", type=int, default=256,
                     help="boxes of the batched-ensemble leg (0 skips it)")
     ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--legs", default="shear,darcy,batch",
+                    help="comma list of legs to run: shear (the headline), darcy, batch")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -442,6 +450,20 @@ def main():
         # replicas only: every rank runs the same single-GPU workload; the
         # timing is the max over ranks (see run_distributed)
         return run_distributed(args, rank, world)
+    legs = set(args.legs.split(","))
+    if "shear" not in legs:
+        # a single side leg (profiling runs): its own JSON object
+        out = {}
+        if "darcy" in legs and args.darcy_steps > 0:
+            out["darcy"] = darcy_leg(args)
+        if "batch" in legs and args.batch_boxes > 0:
+            out["batch"] = batch_leg(args)
+        print(json.dumps(out), flush=True)
+        return 0
+    if "darcy" not in legs:
+        args.darcy_steps = 0
+    if "batch" not in legs:
+        args.batch_boxes = 0
     print(json.dumps(run_gpu(args)), flush=True)
     return 0
 

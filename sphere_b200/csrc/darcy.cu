@@ -12,6 +12,7 @@
 // applied on the device -- no host round trip per check.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -49,6 +50,17 @@ struct DarcyCtl {
     long long ws_picked;
 };
 
+// Barrier state of the cooperative Jacobi kernel: arrival counter and the
+// generation the waiters poll on separate 128-byte lines; launches of more
+// than 64 blocks arrive through 16 sub-counters first.
+struct JacobiSync {
+    unsigned count;
+    unsigned pad0[31];
+    unsigned gen;
+    unsigned pad1[31];
+    unsigned sub[16][32];
+};
+
 struct DarcyDev {
     DarcyParams D;
     size_t ng;
@@ -58,6 +70,7 @@ struct DarcyDev {
     double4 *f_p;                          // original particle order
     double *gather;                        // nx*ny*nz*3 doubles for field reads
     DarcyCtl *ctl;
+    JacobiSync *jsync;
     double host_wall0_w;
     long long conv_iters_last;
     // learned warm start (null when off)
@@ -438,23 +451,35 @@ __global__ void k_first_solution(DarcyParams D, DarcyFields F, const double *p, 
     dp_expl[didx(D, x, y, z)] = dp_of(D, F, p, dctl->wall0_iz, dt, x, y, z);
 }
 
-// Bounded grid barrier for the cooperative Jacobi kernel.
-__device__ bool darcy_barrier(DarcyCtl *ctl, unsigned nblocks)
+// Bounded grid barrier for the cooperative Jacobi kernel: after ~2^24 polls
+// it records DERR_TIMEOUT and returns false.
+__device__ bool darcy_barrier(JacobiSync *js, DarcyCtl *ctl, unsigned nblocks)
 {
     __syncthreads();
     __shared__ int ok;
     if (threadIdx.x == 0) {
-        volatile unsigned *gen = &ctl->barrier_gen;
-        unsigned g = *gen;
+        volatile unsigned *gen = &js->gen;
+        const unsigned g = *gen;
         __threadfence();
-        unsigned arrived = atomicAdd(&ctl->barrier_count, 1u);
-        ok = 1;
-        if (arrived == nblocks - 1) {
-            ctl->barrier_count = 0;
-            __threadfence();
-            atomicAdd(&ctl->barrier_gen, 1u);
+        bool last;
+        if (nblocks > 64) {
+            const unsigned s = blockIdx.x % 16u, members = (nblocks - s + 15u) / 16u;
+            last = false;
+            if (atomicAdd(&js->sub[s][0], 1u) == members - 1u) {
+                js->sub[s][0] = 0;
+                __threadfence();
+                last = atomicAdd(&js->count, 1u) == 15u;
+            }
         } else {
-            unsigned spins = 0;
+            last = atomicAdd(&js->count, 1u) == nblocks - 1u;
+        }
+        ok = 1;
+        if (last) {
+            js->count = 0;
+            __threadfence();
+            atomicAdd(&js->gen, 1u);
+        } else {
+            unsigned spins = 0, nap = 32;
             while (*gen == g) {
                 if (++spins > (1u << 24)) {
                     atomicCAS(&ctl->err, 0, DERR_TIMEOUT);
@@ -462,7 +487,8 @@ __device__ bool darcy_barrier(DarcyCtl *ctl, unsigned nblocks)
                     break;
                 }
                 if (((volatile int *)&ctl->err)[0] == DERR_TIMEOUT) { ok = 0; break; }
-                __nanosleep(32);
+                __nanosleep(nap);
+                if (nap < 256) nap <<= 1;
             }
         }
         __threadfence();
@@ -476,7 +502,7 @@ __device__ bool darcy_barrier(DarcyCtl *ctl, unsigned nblocks)
 // residual (p_new - p)/(p + 1e-16); stop when the maximum |residual| is at
 // most the tolerance at an iteration divisible by 10.
 __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, double *pa, double *pb,
-                                                DarcyCtl *ctl, double dt, int exact_stop)
+                                                DarcyCtl *ctl, JacobiSync *js, double dt, int exact_stop)
 {
     __shared__ double wmax[8];
     const unsigned G = gridDim.x;
@@ -492,7 +518,7 @@ __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, do
         ctl->res_bits[1] = 0ull;
         ctl->res_bits[2] = 0ull;
     }
-    if (!darcy_barrier(ctl, G)) return;
+    if (!darcy_barrier(js, ctl, G)) return;
     for (unsigned nijac = 0; nijac < D.maxiter && !stop; ++nijac) {
         double lmax = 0.0;
         bool nan = false;
@@ -527,7 +553,7 @@ __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, do
             atomicMax(&ctl->res_bits[nijac % 3], (unsigned long long)__double_as_longlong(bm));
         }
         if (__syncthreads_or(nan) && threadIdx.x == 0) atomicExch(&ctl->res_bits[nijac % 3], ~0ull);
-        if (!darcy_barrier(ctl, G)) return;
+        if (!darcy_barrier(js, ctl, G)) return;
         const unsigned long long bits = ((volatile unsigned long long *)ctl->res_bits)[nijac % 3];
         // slot (nijac + 2) % 3 was last read before this barrier and is next
         // written after the following one
@@ -680,9 +706,10 @@ int Engine::darcy_init()
     Dd.f_p = dalloc<double4>(hs.np);
     Dd.gather = dalloc<double>(3 * nx * ny * nz);
     Dd.ctl = dalloc<DarcyCtl>(1);
+    Dd.jsync = dalloc<JacobiSync>(1);
     if (!Dd.p || !Dd.p2 || !Dd.p_old || !Dd.dp_expl || !Dd.phi || !Dd.dphi || !Dd.k ||
         !Dd.div_v_p || !Dd.v || !Dd.vp_avg || !Dd.grad_p || !Dd.grad_k || !Dd.p_constant ||
-        !Dd.f_p || !Dd.gather || !Dd.ctl) return fail(ST_CUDA, "device allocation failed (Darcy)");
+        !Dd.f_p || !Dd.gather || !Dd.ctl || !Dd.jsync) return fail(ST_CUDA, "device allocation failed (Darcy)");
     std::vector<double> p(ng, 0.0), phi(ng, 0.0), dphi(ng, 0.0), v(3 * ng, 0.0);
     std::vector<int> pc(ng, 0);
     for (size_t z = 0; z < nz; ++z)
@@ -713,7 +740,11 @@ int Engine::darcy_init()
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi, 256, 0);
     if (per_sm < 1) return fail(ST_CUDA, "Jacobi kernel cannot be resident");
-    jacobi_grid = sms * (per_sm < 4 ? per_sm : 4);
+    // resident blocks per SM of the Jacobi launch (two by default; the
+    // variable SPHB_JACOBI_BLOCKS_PER_SM overrides it for tuning runs)
+    int bps = 2;
+    if (const char *env = std::getenv("SPHB_JACOBI_BLOCKS_PER_SM")) bps = std::max(1, std::atoi(env));
+    jacobi_grid = sms * (per_sm < bps ? per_sm : bps);
     unsigned need = cells_blocks(D);
     if ((unsigned)jacobi_grid > need) jacobi_grid = (int)need;
     if (warm_start) {
@@ -808,7 +839,7 @@ cudaError_t Engine::enqueue_fluid()
     double dt = P.dt;
     int exact = darcy_exact_stop;
     void *args[] = {(void *)&D, (void *)&F, (void *)&Dd.p, (void *)&Dd.p2, (void *)&Dd.ctl,
-                    (void *)&dt, (void *)&exact};
+                    (void *)&Dd.jsync, (void *)&dt, (void *)&exact};
     e = cudaLaunchCooperativeKernel((void *)k_jacobi, dim3(jacobi_grid), dim3(256), args, 0, stream);
     if (e != cudaSuccess) return e;
     k_final_pressure<<<cb, 256, 0, stream>>>(D, Dd.ctl, Dd.p, Dd.p2, Dd.ng);

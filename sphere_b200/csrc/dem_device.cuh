@@ -386,23 +386,15 @@ struct ContactOut {
 };
 
 // Contact search + forces of sorted particle k (topology and interact of
-// the reference, walls included).  srow / skb are the thread's slot scratch
-// in shared memory (entry i at [i * B + t]): the partner's original index
-// and, for partners found overlapping this step, its sorted index.
+// the reference, walls included).  srow is the thread's slot scratch in
+// shared memory (entry i at srow[i * B + t]: the partner's original index).
 // Returns false after raising a capacity error.
 // PREC 0: faithful FP64, 1: FP64, 2: mixed (FP64 overlap, FP32 contact law,
 // FP64 accumulation).
-//
-// Every overlapping pair is in the neighbour list and the topology visit
-// computes exactly the overlap the reference's interact recomputes (same
-// operands, same operation order), so a slot is in contact this step iff
-// topology hit it: interact evaluates the hit slots in slot order with the
-// partner's sorted index at hand, and clears the other occupied slots
-// without loading their partners.
 template <int PREC, int MODEL>
 __device__ __forceinline__ bool contact_particle(const DevParams &P, const DevState &S, unsigned k,
-                                                 uint32_t *srow, uint32_t *skb, unsigned B,
-                                                 unsigned t, ContactOut &out)
+                                                 uint32_t *srow, unsigned B, unsigned t,
+                                                 ContactOut &out)
 {
     constexpr int TP = PREC == 2 ? 1 : PREC;  // precision of overlap tests
     const unsigned NC = P.nc;
@@ -420,7 +412,7 @@ __device__ __forceinline__ bool contact_particle(const DevParams &P, const DevSt
     if (MODEL == 2) {
         const size_t rowbase = (size_t)o * NC;
         uint64_t mask = S.occ[o];
-        uint64_t written = 0, hit = 0;
+        uint64_t written = 0;
         {
             uint64_t m = mask;
             while (m) {
@@ -448,10 +440,8 @@ __device__ __forceinline__ bool contact_particle(const DevParams &P, const DevSt
                     return false;
                 }
                 srow[cpos * B + t] = b_orig;
-                skb[cpos * B + t] = b;
                 mask |= 1ull << cpos;
                 written |= 1ull << cpos;
-                hit |= 1ull << cpos;
                 S.dmcode[rowbase + cpos] = dm_encode(sx, sy);
                 ++nc;
             }
@@ -469,42 +459,38 @@ __device__ __forceinline__ bool contact_particle(const DevParams &P, const DevSt
             for_each_cell_candidate(P, S, k, xa, visit);
         }
         if (!ok) return false;
-        // --- interact: occupied slots that were not hit are no longer in
-        // contact; the hit slots get forces in slot order ---
-        {
-            uint64_t gone = mask & ~hit;
-            while (gone) {
-                const int i = __ffsll((long long)gone) - 1;
-                gone &= gone - 1;
-                const size_t mempos = rowbase + i;
-                mask &= ~(1ull << i);
-                written |= 1ull << i;
-                if constexpr (PREC == 2) S.delta_t_f[mempos] = make_float4(0.f, 0.f, 0.f, 0.f);
-                else S.delta_t[mempos] = make_double4(0.0, 0.0, 0.0, 0.0);
-            }
-        }
-        uint64_t m = hit;
+        // --- interact, history contacts in slot order ---
+        uint64_t m = mask;
         while (m) {
             const int i = __ffsll((long long)m) - 1;
             m &= m - 1;
+            const unsigned b_orig = srow[i * B + t];
+            if (b_orig >= P.np) { raise_err(S.ctl, DERR_CAPACITY, (int)o); return false; }
             const size_t mempos = rowbase + i;
-            const unsigned kb = skb[i * B + t];
             V3 dm = dm_decode(P, S.dmcode[mempos]);
+            unsigned kb = S.pos_of[b_orig];
             double4 xb = S.x[kb];
             double rb = xb.w;
             V3 x_ab = mk3(xa.x - xb.x + dm.x, xa.y - xb.y + dm.y, xa.z - xb.z + dm.z);
             double len = vlen<TP>(x_ab);
             double delta_n = len - (ra + rb);
-            if constexpr (PREC == 2) {
-                float4 h = S.delta_t_f[mempos];
-                mixed_pair(P, F, T, es_dot, ev_dot, p, S.vel_f[k], S.angvel_f[k], S.vel_f[kb],
-                           S.angvel_f[kb], h, ra, rb, x_ab, len, delta_n);
-                S.delta_t_f[mempos] = h;
+            if (delta_n < 0.0) {
+                if constexpr (PREC == 2) {
+                    float4 h = S.delta_t_f[mempos];
+                    mixed_pair(P, F, T, es_dot, ev_dot, p, S.vel_f[k], S.angvel_f[k], S.vel_f[kb],
+                               S.angvel_f[kb], h, ra, rb, x_ab, len, delta_n);
+                    S.delta_t_f[mempos] = h;
+                } else {
+                    V3 dt_new = contact_linear<PREC>(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a,
+                                                     S.vel[kb], xyz(S.angvel[kb]),
+                                                     S.delta_t[mempos], ra, rb, x_ab, len, delta_n);
+                    S.delta_t[mempos] = make_double4(dt_new.x, dt_new.y, dt_new.z, 0.0);
+                }
             } else {
-                V3 dt_new = contact_linear<PREC>(P, F, T, es_dot, ev_dot, p, vel_a, angvel_a,
-                                                 S.vel[kb], xyz(S.angvel[kb]), S.delta_t[mempos],
-                                                 ra, rb, x_ab, len, delta_n);
-                S.delta_t[mempos] = make_double4(dt_new.x, dt_new.y, dt_new.z, 0.0);
+                mask &= ~(1ull << i);
+                written |= 1ull << i;
+                if constexpr (PREC == 2) S.delta_t_f[mempos] = make_float4(0.f, 0.f, 0.f, 0.f);
+                else S.delta_t[mempos] = make_double4(0.0, 0.0, 0.0, 0.0);
             }
         }
         if (written) {
@@ -626,14 +612,12 @@ __device__ __forceinline__ void nl_build_particle(const DevParams &P, const DevS
 template <int PREC, int MODEL>
 __global__ void __launch_bounds__(128, SPHB_CONTACT_MINB) k_contacts(DevParams P, DevState S)
 {
-    extern __shared__ uint32_t srow[];   // blockDim * nc slot partners, then as many sorted indices
+    extern __shared__ uint32_t srow[];   // blockDim * nc slot partners
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k == 0 && S.ctl->nl_rebuild) S.ctl->nl_rebuild = 0;  // k_nl_build has run
     if (S.ctl->err || k >= P.np) return;
     ContactOut c;
-    if (!contact_particle<PREC, MODEL>(P, S, k, srow, srow + (size_t)blockDim.x * P.nc, blockDim.x,
-                                       threadIdx.x, c))
-        return;
+    if (!contact_particle<PREC, MODEL>(P, S, k, srow, blockDim.x, threadIdx.x, c)) return;
     contact_writeback(P, S, k, c);
 }
 

@@ -265,10 +265,10 @@ cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cud
     if (e != cudaSuccess) return e;
     dim3 grid(blocks_for(P.np, B));
     if (P.contactmodel == 2) {
-        size_t smem = 2 * (size_t)B * P.nc * sizeof(uint32_t);
+        size_t smem = (size_t)B * P.nc * sizeof(uint32_t);
         static bool attr = false;
         if (!attr) {
-            int mx = (int)(2 * (size_t)B * 64 * sizeof(uint32_t));
+            int mx = (int)((size_t)B * 64 * sizeof(uint32_t));
             cudaFuncSetAttribute(k_contacts<0, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
             cudaFuncSetAttribute(k_contacts<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
             attr = true;

@@ -15,11 +15,11 @@ cudaError_t launch_contacts_mixed(const DevParams &P, const DevState &S, cudaStr
     if (e != cudaSuccess) return e;
     dim3 grid((P.np + B - 1) / B);
     if (P.contactmodel == 2) {
-        size_t smem = 2 * (size_t)B * P.nc * sizeof(uint32_t);
+        size_t smem = (size_t)B * P.nc * sizeof(uint32_t);
         static bool attr = false;
         if (!attr) {
             cudaFuncSetAttribute(k_contacts<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(2 * (size_t)B * 64 * sizeof(uint32_t)));
+                                 (int)((size_t)B * 64 * sizeof(uint32_t)));
             attr = true;
         }
         k_contacts<2, 2><<<grid, B, smem, st>>>(P, S);

@@ -150,9 +150,8 @@ __device__ __forceinline__ bool group_barrier(GroupSync *g, GroupTree *tree, uns
     return ok != 0;
 }
 
-// Dynamic shared memory: the slot rows (2 * NT * nc u32: partners and their
-// sorted indices, at least 16 KB so the same space stages the ordered
-// wall-force sum).  NT threads per block,
+// Dynamic shared memory: the slot rows (NT * nc u32, at least 16 KB so the
+// same space stages the ordered wall-force sum).  NT threads per block,
 // MINB resident blocks per SM (register budget 65536 / (NT * MINB)).
 template <int PREC, int MODEL, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_persistent(BatchArgs A)
@@ -258,8 +257,7 @@ __global__ void __launch_bounds__(NT, MINB) k_persistent(BatchArgs A)
             for (unsigned k = gtid; k < P.np; k += gstride) {
                 if (nl) nl_build_particle(P, S, k);
                 ContactOut c;
-                if (!contact_particle<PREC, MODEL>(P, S, k, srow, srow + (size_t)B * P.nc, B, t, c))
-                    continue;
+                if (!contact_particle<PREC, MODEL>(P, S, k, srow, B, t, c)) continue;
                 contact_writeback(P, S, k, c);
                 integrate_particle(P, S, k, make_double4(c.F.x, c.F.y, c.F.z, 0.0f),
                                    make_double4(c.T.x, c.T.y, c.T.z, 0.0f), clk, S.x_nx, S.vel_nx,

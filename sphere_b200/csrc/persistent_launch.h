@@ -50,7 +50,7 @@ inline void set_sync_args(BatchArgs &A, unsigned char *sync)
 // dynamic shared memory of a launch: slot rows, at least the 16 KB stage
 inline size_t persistent_smem(int threads, unsigned nc)
 {
-    size_t rows = 2 * (size_t)threads * nc * 4;
+    size_t rows = (size_t)threads * nc * 4;
     return rows > 16384 ? rows : 16384;
 }
 
