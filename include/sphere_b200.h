@@ -107,6 +107,7 @@ typedef enum sph_field {
     SPH_F_BONDS,        /* nb0 x 2 u32 */
     SPH_F_BONDS_DELTA,  /* nb0 x 4 doubles (t.x, t.y, t.z, n) */
     SPH_F_BONDS_OMEGA,
+    SPH_F_VELOCITY_STATE, /* 1 int64: rate-state velocity step state (device.cu:2461-2469) */
     SPH_F_COUNT
 } sph_field;
 
@@ -180,6 +181,35 @@ int sph_set(sph_engine *e, sph_field f, const void *src, size_t bytes);
 int sph_write_bin(sph_engine *e, const char *path);
 
 int sph_get_info(sph_engine *e, sph_info *info);
+
+/* Energy sum of the current state, computed on the device.  Replaces
+ * sim.energy(method) (python/sphere.py:4311-4380); method is one of "pot",
+ * "kin", "rot", "shear", "shearrate", "visc_n", "visc_n_rate", "bondpot"
+ * with the reference's formulas (its "bondpot" multiplies each bond's
+ * tangential factors by the norm of the whole delta_t / omega_t arrays,
+ * and so does this).  An unknown method is SPH_ERR_ARG, as the reference
+ * raises. */
+int sph_energy(sph_engine *e, const char *method, double *out);
+
+/* Porosity in z_slices horizontal slabs from z = 0 to the upper wall
+ * (L_z without walls); z_pos and porosity receive z_slices values each.
+ * Replaces DEM::porosity (src/sphere.cpp:487-605), the `porosity` program
+ * behind sim.porosity() (python/sphere.py:4437-4480), with its case
+ * analysis and its slice-height check against twice the radius of the
+ * last particle (SPH_ERR_ARG where the reference exits). */
+int sph_porosity(sph_engine *e, int z_slices, double *z_pos, double *porosity);
+
+/* Overlapping particle pairs: i < j (original indices), separation
+ * |x_j - x_i| - (r_i + r_j) < 0, both fixvel flags zero, no periodic
+ * images -- the list of DEM::findOverlaps (src/sphere.cpp:677-725) that
+ * `sphere --contacts` prints (src/sphere.cpp:904-913) for
+ * sim.findOverlaps() (python/sphere.py:4868-4883), in the same order
+ * (i, then j ascending) with the same FP64 separations.  *count receives
+ * the number of pairs.  With pairs and delta NULL only the count is
+ * computed; otherwise pairs (2 x capacity u32) and delta (capacity
+ * doubles) are filled, or SPH_ERR_ARG is returned when capacity < count. */
+int sph_overlaps(sph_engine *e, uint32_t *pairs, double *delta, uint64_t capacity,
+                 uint64_t *count);
 
 /* Message for the last non-zero status of this handle (never NULL). */
 const char *sph_last_error(sph_engine *e);

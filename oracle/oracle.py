@@ -169,6 +169,12 @@ def ref_lib():
                                  ctypes.c_void_p, ctypes.c_size_t]
         _ref.ref_get.restype = ctypes.c_long
         _ref.ref_close.argtypes = [ctypes.c_void_p]
+        _ref.ref_porosity.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_void_p]
+        _ref.ref_porosity.restype = ctypes.c_long
+        _ref.ref_overlaps.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_long]
+        _ref.ref_overlaps.restype = ctypes.c_long
     return _ref
 
 
@@ -192,6 +198,23 @@ class Reference:
 
     def write_bin(self, path):
         return ref_lib().ref_write(self._h, os.fsencode(path))
+
+    def porosity(self, slices):
+        """DEM::porosity (the `porosity` program): (z_pos, porosity)."""
+        z = numpy.zeros(slices)
+        p = numpy.zeros(slices)
+        n = ref_lib().ref_porosity(self._h, int(slices), z.ctypes.data, p.ctypes.data)
+        if n != slices:
+            raise OracleError(f"porosity printed {n} of {slices} lines")
+        return z, p
+
+    def overlaps(self):
+        """DEM::findOverlaps: (pairs M x 2, separations M)."""
+        m = ref_lib().ref_overlaps(self._h, None, None, 0)
+        pairs = numpy.zeros((m, 2), dtype=numpy.uint32)
+        d = numpy.zeros(m)
+        ref_lib().ref_overlaps(self._h, pairs.ctypes.data, d.ctypes.data, m)
+        return pairs, d
 
     def close(self):
         if self._h:

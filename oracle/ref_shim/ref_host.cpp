@@ -17,6 +17,8 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <iostream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -529,6 +531,48 @@ long ref_get(void *h, const char *name, void *dst, size_t bytes)
     if (!dst || bytes < need) return (long)need;
     std::memcpy(dst, src, need);
     return 0;
+}
+
+/* DEM::porosity (sphere.cpp:487-605) on the current state.  It prints
+ * "z\tporosity" lines; they are read back at full precision.  Returns the
+ * number of lines parsed.  The caller keeps z_slices valid: the reference
+ * exits on a slice height below twice the last radius. */
+long ref_porosity(void *h, int z_slices, double *z_pos, double *porosity)
+{
+    RefRun *r = (RefRun *)h;
+    r->dem->transferFromGlobalDeviceMemory();
+    std::ostringstream text;
+    std::streambuf *old = std::cout.rdbuf(text.rdbuf());
+    std::streamsize prec = std::cout.precision(17);
+    r->dem->porosity(z_slices);
+    std::cout.precision(prec);
+    std::cout.rdbuf(old);
+    std::istringstream in(text.str());
+    long n = 0;
+    double z, p;
+    while (n < z_slices && in >> z >> p) {
+        z_pos[n] = z;
+        porosity[n] = p;
+        ++n;
+    }
+    return n;
+}
+
+/* DEM::findOverlaps (sphere.cpp:677-725) on the current state: writes up
+ * to cap pairs and separations, returns the number found. */
+long ref_overlaps(void *h, unsigned *pairs, double *delta, long cap)
+{
+    RefRun *r = (RefRun *)h;
+    r->dem->transferFromGlobalDeviceMemory();
+    std::vector<std::vector<unsigned int>> ij;
+    std::vector<Float> d;
+    r->dem->findOverlaps(ij, d);
+    for (long q = 0; q < (long)ij.size() && q < cap; ++q) {
+        pairs[2 * q] = ij[q][0];
+        pairs[2 * q + 1] = ij[q][1];
+        delta[q] = d[q];
+    }
+    return (long)ij.size();
 }
 
 void ref_close(void *h)

@@ -61,9 +61,24 @@ struct JacobiSync {
     unsigned sub[16][32];
 };
 
+// Constants of one solve's Jacobi update, independent of the iterate and
+// formed once per fluid step with the reference's operation order, so the
+// iteration reproduces updateDarcySolution's arithmetic bit for bit while
+// reading 9 values per cell instead of 24 and dividing 9 times fewer.
+struct JacobiCoef {
+    const double *cf;      // 6 x ng: face factors 2 k_nb k / (k_nb + k): xp, xn, yp, yn, zp, zn
+    const double *a;       // ndt / (beta_f phi mu)
+    const double *src;     // ndt / (beta_f phi (1 - phi)) * (dphi / ndt + v_p . grad phi)
+    const double *base;    // p_old + (1 - epsilon) dp_expl
+    const unsigned char *fixed;  // 1 where the pressure change is forced to 0
+    unsigned long long ng;
+};
+
 struct DarcyDev {
     DarcyParams D;
     size_t ng;
+    double *cf = nullptr, *ca = nullptr, *csrc = nullptr, *cbase = nullptr;
+    unsigned char *cfixed = nullptr;
     double *p, *p2, *p_old, *dp_expl, *phi, *dphi, *k, *div_v_p;
     double *v, *vp_avg, *grad_p, *grad_k;  // 3 doubles per cell
     int *p_constant;
@@ -451,6 +466,72 @@ __global__ void k_first_solution(DarcyParams D, DarcyFields F, const double *p, 
     dp_expl[didx(D, x, y, z)] = dp_of(D, F, p, dctl->wall0_iz, dt, x, y, z);
 }
 
+// The iterate-independent parts of dp_of for every interior cell
+// (darcy.cuh:1602-1799), written for k_jacobi.
+__global__ void k_jacobi_coef(DarcyParams D, DarcyFields F, const DarcyCtl *dctl, double dt,
+                              double *cf, double *ca, double *csrc, double *cbase,
+                              unsigned char *cfixed, unsigned long long ng)
+{
+    int x, y, z;
+    if (!cell_of_thread(D, x, y, z)) return;
+    const int nx = D.nx, ny = D.ny, nz = D.nz;
+    const double dx = D.dx, dy = D.dy, dz = D.dz;
+    const unsigned c = didx(D, x, y, z);
+    const unsigned wall0_iz = dctl->wall0_iz;
+    const double phi_xn = F.phi[didx(D, x - 1, y, z)], phi = F.phi[c];
+    const double phi_xp = F.phi[didx(D, x + 1, y, z)], phi_yn = F.phi[didx(D, x, y - 1, z)];
+    const double phi_yp = F.phi[didx(D, x, y + 1, z)], phi_zn = F.phi[didx(D, x, y, z - 1)];
+    const double phi_zp = F.phi[didx(D, x, y, z + 1)];
+    const double dphi = F.dphi[c];
+    const double *vp = &F.vp_avg[3 * (size_t)c];
+    const double k_xn = F.k[didx(D, x - 1, y, z)], k = F.k[c], k_xp = F.k[didx(D, x + 1, y, z)];
+    const double k_yn = F.k[didx(D, x, y - 1, z)], k_yp = F.k[didx(D, x, y + 1, z)];
+    const double k_zn = F.k[didx(D, x, y, z - 1)], k_zp = F.k[didx(D, x, y, z + 1)];
+    const double gx = (phi_xp - phi_xn) / (dx + dx), gy = (phi_yp - phi_yn) / (dy + dy),
+                 gz = (phi_zp - phi_zn) / (dz + dz);
+    cf[c] = 2. * k_xp * k / (k_xp + k);
+    cf[ng + c] = 2. * k_xn * k / (k_xn + k);
+    cf[2 * ng + c] = 2. * k_yp * k / (k_yp + k);
+    cf[3 * ng + c] = 2. * k_yn * k / (k_yn + k);
+    cf[4 * ng + c] = 2. * k_zp * k / (k_zp + k);
+    cf[5 * ng + c] = 2. * k_zn * k / (k_zn + k);
+    const double ndt = D.ndem * dt;
+    ca[c] = ndt / (D.beta_f * phi * D.mu);
+    csrc[c] = (ndt / (D.beta_f * phi * (1.0 - phi))) * (dphi / ndt + (vp[0] * gx + vp[1] * gy + vp[2] * gz));
+    const double epsilon = 0.5;
+    cbase[c] = F.p_old[c] + (1.0 - epsilon) * F.dp_expl[c];
+    cfixed[c] = ((D.bc_bot == 0 && z == 0) || (D.bc_top == 0 && z == nz - 1) ||
+                 ((unsigned)z >= wall0_iz && D.bc_top == 0) || (D.bc_xn == 0 && x == 0) ||
+                 (D.bc_xp == 0 && x == nx - 1) || (D.bc_yn == 0 && y == 0) ||
+                 (D.bc_yp == 0 && y == nx - 1) || F.p_constant[c] == 1) ? 1 : 0;
+    (void)ny;
+}
+
+// dp_of from the per-solve constants: the same operations in the same
+// order on the same values.
+__device__ __forceinline__ double dp_fast(const DarcyParams &D, const JacobiCoef &C, const double *pf,
+                                          unsigned c, int x, int y, int z)
+{
+    if (C.fixed[c]) return 0.0;
+    const unsigned sx = (unsigned)D.nx + 2u, sxy = sx * ((unsigned)D.ny + 2u);
+    const double dx = D.dx, dy = D.dy, dz = D.dz;
+    const double p = pf[c];
+    double p_xn = pf[c - 1], p_xp = pf[c + 1], p_yn = pf[c - sx], p_yp = pf[c + sx];
+    double p_zn = pf[c - sxy], p_zp = pf[c + sxy];
+    if (x == 0 && D.bc_xn == 1) p_xn = p;
+    if (x == D.nx - 1 && D.bc_xp == 1) p_xp = p;
+    if (y == 0 && D.bc_yn == 1) p_yn = p;
+    if (y == D.ny - 1 && D.bc_yp == 1) p_yp = p;
+    if (z == 0 && D.bc_bot == 1) p_zn = p;
+    if (z == D.nz - 1 && D.bc_top == 1) p_zp = p;
+    const size_t ng = C.ng;
+    const double div_k_grad_p =
+        (C.cf[c] * (p_xp - p) / dx - C.cf[ng + c] * (p - p_xn) / dx) / dx +
+        (C.cf[2 * ng + c] * (p_yp - p) / dy - C.cf[3 * ng + c] * (p - p_yn) / dy) / dy +
+        (C.cf[4 * ng + c] * (p_zp - p) / dz - C.cf[5 * ng + c] * (p - p_zn) / dz) / dz;
+    return C.a[c] * div_k_grad_p - C.src[c];
+}
+
 // Bounded grid barrier for the cooperative Jacobi kernel: after ~2^24 polls
 // it records DERR_TIMEOUT and returns false.
 __device__ bool darcy_barrier(JacobiSync *js, DarcyCtl *ctl, unsigned nblocks)
@@ -501,14 +582,13 @@ __device__ bool darcy_barrier(JacobiSync *js, DarcyCtl *ctl, unsigned nblocks)
 // p_new = p_old + 0.5 dp_expl + 0.5 dp_impl(p); p_new <- 0.95 p + 0.05 p_new;
 // residual (p_new - p)/(p + 1e-16); stop when the maximum |residual| is at
 // most the tolerance at an iteration divisible by 10.
-__global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, double *pa, double *pb,
-                                                DarcyCtl *ctl, JacobiSync *js, double dt, int exact_stop)
+__global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, JacobiCoef C, double *pa,
+                                                double *pb, DarcyCtl *ctl, JacobiSync *js, int exact_stop)
 {
     __shared__ double wmax[8];
     const unsigned G = gridDim.x;
     const unsigned n = (unsigned)D.nx * D.ny * D.nz;
     const unsigned stride = G * blockDim.x;
-    const unsigned wall0_iz = ctl->wall0_iz;
     double *cur = pa, *nxt = pb;
     long long nijac_done = 0;
     long long converged_at = -1;
@@ -526,10 +606,10 @@ __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, do
             const int x = (int)(i % D.nx), y = (int)((i / D.nx) % D.ny),
                       z = (int)(i / ((unsigned)D.nx * D.ny));
             const unsigned c = didx(D, x, y, z);
-            const double dp_impl = dp_of(D, F, cur, wall0_iz, dt, x, y, z);
+            const double dp_impl = dp_fast(D, C, cur, c, x, y, z);
             const double epsilon = 0.5, theta = 0.05;
             const double p = cur[c];
-            double p_new = F.p_old[c] + (1.0 - epsilon) * F.dp_expl[c] + epsilon * dp_impl;
+            double p_new = C.base[c] + epsilon * dp_impl;
             p_new = p * (1.0 - theta) + p_new * theta;
             const double res = (p_new - p) / (p + 1.0e-16);
             const double a = fabs(res);
@@ -707,9 +787,12 @@ int Engine::darcy_init()
     Dd.gather = dalloc<double>(3 * nx * ny * nz);
     Dd.ctl = dalloc<DarcyCtl>(1);
     Dd.jsync = dalloc<JacobiSync>(1);
+    Dd.cf = dalloc<double>(6 * ng); Dd.ca = dalloc<double>(ng); Dd.csrc = dalloc<double>(ng);
+    Dd.cbase = dalloc<double>(ng); Dd.cfixed = dalloc<unsigned char>(ng);
     if (!Dd.p || !Dd.p2 || !Dd.p_old || !Dd.dp_expl || !Dd.phi || !Dd.dphi || !Dd.k ||
         !Dd.div_v_p || !Dd.v || !Dd.vp_avg || !Dd.grad_p || !Dd.grad_k || !Dd.p_constant ||
-        !Dd.f_p || !Dd.gather || !Dd.ctl || !Dd.jsync) return fail(ST_CUDA, "device allocation failed (Darcy)");
+        !Dd.f_p || !Dd.gather || !Dd.ctl || !Dd.jsync || !Dd.cf || !Dd.ca || !Dd.csrc ||
+        !Dd.cbase || !Dd.cfixed) return fail(ST_CUDA, "device allocation failed (Darcy)");
     std::vector<double> p(ng, 0.0), phi(ng, 0.0), dphi(ng, 0.0), v(3 * ng, 0.0);
     std::vector<int> pc(ng, 0);
     for (size_t z = 0; z < nz; ++z)
@@ -816,6 +899,8 @@ cudaError_t Engine::enqueue_fluid()
     k_ghost<1><<<cb, 256, 0, stream>>>(D, Dd.p);
     DarcyFields F{Dd.phi, Dd.dphi, Dd.k, Dd.vp_avg, Dd.p_old, Dd.dp_expl, Dd.p_constant};
     k_first_solution<<<cb, 256, 0, stream>>>(D, F, Dd.p, Dd.dp_expl, Dd.ctl, P.dt);
+    k_jacobi_coef<<<cb, 256, 0, stream>>>(D, F, Dd.ctl, P.dt, Dd.cf, Dd.ca, Dd.csrc, Dd.cbase, Dd.cfixed,
+                                          (unsigned long long)Dd.ng);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (Dd.ws) {
         // learned initial iterate; the previous-step guess stays unless the
@@ -836,10 +921,10 @@ cudaError_t Engine::enqueue_fluid()
     // the second buffer starts as a copy (its ghost faces are read too)
     if ((e = cudaMemcpyAsync(Dd.p2, Dd.p, Dd.ng * 8, cudaMemcpyDeviceToDevice, stream)) != cudaSuccess)
         return e;
-    double dt = P.dt;
     int exact = darcy_exact_stop;
-    void *args[] = {(void *)&D, (void *)&F, (void *)&Dd.p, (void *)&Dd.p2, (void *)&Dd.ctl,
-                    (void *)&Dd.jsync, (void *)&dt, (void *)&exact};
+    JacobiCoef C{Dd.cf, Dd.ca, Dd.csrc, Dd.cbase, Dd.cfixed, (unsigned long long)Dd.ng};
+    void *args[] = {(void *)&D, (void *)&F, (void *)&C, (void *)&Dd.p, (void *)&Dd.p2, (void *)&Dd.ctl,
+                    (void *)&Dd.jsync, (void *)&exact};
     e = cudaLaunchCooperativeKernel((void *)k_jacobi, dim3(jacobi_grid), dim3(256), args, 0, stream);
     if (e != cudaSuccess) return e;
     k_final_pressure<<<cb, 256, 0, stream>>>(D, Dd.ctl, Dd.p, Dd.p2, Dd.ng);

@@ -438,7 +438,7 @@ int64_t Engine::field_bytes(int f) const
     case SPH_F_DELTA_T: case SPH_F_DISTMOD: return (int64_t)slots * 32;
     case SPH_F_WALLS_NX: case SPH_F_WALLS_MVFD: return (int64_t)hs.nw * 32;
     case SPH_F_WALLS_ACC: return (int64_t)hs.nw * 8;
-    case SPH_F_ITER: return 8;
+    case SPH_F_ITER: case SPH_F_VELOCITY_STATE: return 8;
     case SPH_F_TIME: return 8;
     case SPH_F_BONDS: return (int64_t)hs.nb0 * 8;
     case SPH_F_BONDS_DELTA: case SPH_F_BONDS_OMEGA: return (int64_t)hs.nb0 * 32;
@@ -507,6 +507,13 @@ int Engine::get(int f, void *dst, size_t bytes)
             int rc = poll_errors("get");
             if (rc < 0 && rc != ST_OUTSIDE && rc != ST_CAPACITY) return rc;
             std::memcpy(dst, &last_ctl.t_current, 8);
+            return ST_OK;
+        }
+        case SPH_F_VELOCITY_STATE: {
+            int rc = poll_errors("get");
+            if (rc < 0 && rc != ST_OUTSIDE && rc != ST_CAPACITY) return rc;
+            int64_t v = last_ctl.velocity_state;
+            std::memcpy(dst, &v, 8);
             return ST_OK;
         }
         case SPH_F_BONDS: d2h(S.bonds, (size_t)need); break;
@@ -594,6 +601,38 @@ int Engine::set(int f, const void *src, size_t bytes)
             break;
         case SPH_F_WALLS_NX: e = cudaMemcpyAsync(S.wnx, src, bytes, cudaMemcpyHostToDevice, stream); break;
         case SPH_F_WALLS_MVFD: e = cudaMemcpyAsync(S.wmvfd, src, bytes, cudaMemcpyHostToDevice, stream); break;
+        case SPH_F_WALLS_ACC: e = cudaMemcpyAsync(S.wacc, src, bytes, cudaMemcpyHostToDevice, stream); break;
+        case SPH_F_DISTMOD: {
+            // (dx, dy, 0, r_partner) per slot -> the periodic shift code
+            const double *d = (const double *)src;
+            std::vector<uint8_t> code(bytes / 32);
+            for (size_t i = 0; i < code.size(); ++i) {
+                const double dx = d[4 * i], dy = d[4 * i + 1];
+                code[i] = (uint8_t)((dx > 0.0 ? 1 : 0) | (dx < 0.0 ? 2 : 0) | (dy > 0.0 ? 4 : 0) |
+                                    (dy < 0.0 ? 8 : 0));
+            }
+            e = cudaMemcpyAsync(S.dmcode, code.data(), code.size(), cudaMemcpyHostToDevice, stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            break;
+        }
+        case SPH_F_ITER: case SPH_F_VELOCITY_STATE: {
+            // loop state: DevCtl on the device, the host mirror of the counter
+            int rc = poll_errors("set");
+            if (rc < 0) return rc;
+            int64_t v;
+            std::memcpy(&v, src, 8);
+            if (f == SPH_F_ITER) {
+                if (v < 0) return fail(ST_ARG, "iter must not be negative");
+                long long it = (long long)v;
+                e = cudaMemcpyAsync(&S.ctl->iter, &it, sizeof it, cudaMemcpyHostToDevice, stream);
+                host_iter = v;
+            } else {
+                int vs = (int)v;
+                e = cudaMemcpyAsync(&S.ctl->velocity_state, &vs, sizeof vs, cudaMemcpyHostToDevice, stream);
+            }
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            break;
+        }
         default: return fail(ST_ARG, "field is read-only");
         }
     }
@@ -968,6 +1007,21 @@ int sph_get_info(sph_engine *e, sph_info *info)
     info->resorts = g.last_ctl.resorts;
     g.persist_describe(info);
     return rc;
+}
+
+int sph_energy(sph_engine *e, const char *method, double *out)
+{
+    return e ? e->e->energy(method, out) : SPH_ERR_ARG;
+}
+
+int sph_porosity(sph_engine *e, int z_slices, double *z_pos, double *porosity)
+{
+    return e ? e->e->porosity_profile(z_slices, z_pos, porosity) : SPH_ERR_ARG;
+}
+
+int sph_overlaps(sph_engine *e, uint32_t *pairs, double *delta, uint64_t capacity, uint64_t *count)
+{
+    return e ? e->e->overlaps(pairs, delta, capacity, count) : SPH_ERR_ARG;
 }
 
 const char *sph_last_error(sph_engine *e) { return e ? e->e->err.c_str() : "no engine"; }

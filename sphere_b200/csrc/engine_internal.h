@@ -112,6 +112,11 @@ public:
     void conv_open();
     void conv_close();
 
+    // diagnostics on the resident state (stats.cu)
+    int energy(const char *method, double *out);
+    int porosity_profile(int z_slices, double *z_pos, double *porosity);
+    int overlaps(uint32_t *pairs, double *delta, uint64_t cap, uint64_t *count);
+
     // mixed precision
     int mixed_init();
 

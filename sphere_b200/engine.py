@@ -24,13 +24,14 @@ FIELDS = [
     "contacts", "delta_t", "distmod", "walls_nx", "walls_mvfd", "walls_acc", "iter",
     "time", "darcy_p", "darcy_phi", "darcy_dphi", "darcy_k", "darcy_v", "darcy_f_p",
     "darcy_iters", "darcy_iters_total", "darcy_iters_exact", "darcy_warm", "bonds", "bonds_delta", "bonds_omega",
+    "velocity_state",
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 _VEC4 = {"x", "vel", "angvel", "angpos", "force", "torque", "acc", "angacc", "xyzsum",
          "delta_t", "distmod", "walls_nx", "walls_mvfd", "darcy_f_p", "bonds_delta",
          "bonds_omega"}
 _U32 = {"cellid", "index", "cellstart", "cellend", "contacts", "bonds"}
-_I64 = {"iter", "darcy_iters", "darcy_iters_total", "darcy_iters_exact", "darcy_warm"}
+_I64 = {"iter", "velocity_state", "darcy_iters", "darcy_iters_total", "darcy_iters_exact", "darcy_warm"}
 
 STATUS = {
     0: "ok", 1: "Darcy solve did not converge", -1: "file error", -2: "version",
@@ -115,6 +116,10 @@ def lib() -> ctypes.CDLL:
     L.sph_open_error.restype = ctypes.c_char_p
     L.sph_check_file.argtypes = [ctypes.c_char_p, ctypes.c_int]
     L.sph_check_file.restype = ctypes.c_int
+    L.sph_energy.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
+    L.sph_porosity.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    L.sph_overlaps.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                               ctypes.POINTER(ctypes.c_uint64)]
     L.sph_close.argtypes = [P]
     L.sph_version.restype = ctypes.c_char_p
     # batches
@@ -272,6 +277,46 @@ class Engine:
 
     def write_bin(self, path) -> None:
         self._check(lib().sph_write_bin(self._h, os.fsencode(path)))
+
+    # diagnostics of sphere's sim class, computed on the device
+
+    def energy(self, method) -> float:
+        """sim.energy(method) (python/sphere.py:4311-4380): 'pot', 'kin',
+        'rot', 'shear', 'shearrate', 'visc_n', 'visc_n_rate' or 'bondpot'."""
+        out = ctypes.c_double(0.0)
+        self._check(lib().sph_energy(self._h, str(method).encode(), ctypes.byref(out)))
+        return out.value
+
+    def porosity(self, slices=10):
+        """sim.porosity(slices) (python/sphere.py:4437-4480): returns
+        (porosity, depth), one value per horizontal slab."""
+        z = numpy.empty(int(slices), dtype=numpy.float64)
+        phi = numpy.empty(int(slices), dtype=numpy.float64)
+        self._check(lib().sph_porosity(self._h, int(slices), z.ctypes.data, phi.ctypes.data))
+        return phi, z
+
+    def find_overlaps(self):
+        """sim.findOverlaps() (python/sphere.py:4868-4883): returns (pairs,
+        overlaps), pairs a 2 x M int32 array of particle indices (i < j) and
+        overlaps the M negative separations, in the order `sphere
+        --contacts` prints them."""
+        L = lib()
+        count = ctypes.c_uint64(0)
+        self._check(L.sph_overlaps(self._h, None, None, 0, ctypes.byref(count)))
+        m = int(count.value)
+        pairs = numpy.empty((m, 2), dtype=numpy.uint32)
+        delta = numpy.empty(m, dtype=numpy.float64)
+        if m:
+            self._check(L.sph_overlaps(self._h, pairs.ctypes.data, delta.ctypes.data, m,
+                                       ctypes.byref(count)))
+        return numpy.ascontiguousarray(pairs.T.astype(numpy.int32)), delta
+
+    def coordination_number(self):
+        """Contacts per particle (sim.findCoordinationNumber,
+        python/sphere.py:4885-4894) from the overlap list."""
+        pairs, _ = self.find_overlaps()
+        return (numpy.bincount(pairs[0], minlength=self.np)
+                + numpy.bincount(pairs[1], minlength=self.np))
 
 
 def check_file(path, fluid=False):
