@@ -39,6 +39,11 @@ sys.path.insert(0, ROOT)
 
 INTERVAL = 100          # DEM steps per benchmark step
 N_PARTICLES = 100000
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_contacts<2,2> launch
+# on this workload (mixed precision, N = 1e5), from an ncu --set full
+# capture of that kernel: 46.29 MB read + 2.80 MB written (ncu flushes the
+# caches before the launch)
+CONTACTS_TRAFFIC = 46.29e6 + 2.80e6
 SEED = 1
 
 
@@ -251,7 +256,9 @@ def run_gpu(args):
                 "h2d_bytes_per_step": 3 * 32 * n, "d2h_bytes_per_step": 5 * 32 * n},
         "gpu_launches": timed_launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": CONTACTS_TRAFFIC if precision == "mixed" else None,
+                     "traffic_unit": "DRAM bytes per launch (ncu, cold caches)",
                      "kernel": "k_contacts (contact search + forces)",
                      "bytes_per_particle": bytes_per_particle,
                      "peak_source": peak_kind},

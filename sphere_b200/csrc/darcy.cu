@@ -50,15 +50,21 @@ struct DarcyCtl {
     long long ws_picked;
 };
 
-// Barrier state of the cooperative Jacobi kernel: arrival counter and the
-// generation the waiters poll on separate 128-byte lines; launches of more
-// than 64 blocks arrive through 16 sub-counters first.
+// Synchronisation of the cooperative Jacobi kernel (zeroed before each
+// launch).  Block b owns a contiguous range of cells and publishes in
+// done[b] how many iterations it has completed; an iteration only needs the
+// previous iterate of the cells within one z layer, so a block waits for
+// the few blocks around it instead of the whole grid.  The residual maxima
+// go to a ring of per-iteration slots; the check iterations of the stop rule
+// count their arrivals so every block can read a complete maximum.  Each
+// counter has its own 128-byte line.
+constexpr unsigned kJacobiMaxBlocks = 1024;
+constexpr unsigned kJacobiRing = 64;     // residual slots (iterations mod 64)
+constexpr unsigned kJacobiChecks = 8;    // arrival counters (check index mod 8)
 struct JacobiSync {
-    unsigned count;
-    unsigned pad0[31];
-    unsigned gen;
-    unsigned pad1[31];
-    unsigned sub[16][32];
+    unsigned long long ring[kJacobiRing];
+    unsigned arrive[kJacobiChecks][32];
+    unsigned done[kJacobiMaxBlocks][32];
 };
 
 // Constants of one solve's Jacobi update, independent of the iterate and
@@ -532,77 +538,130 @@ __device__ __forceinline__ double dp_fast(const DarcyParams &D, const JacobiCoef
     return C.a[c] * div_k_grad_p - C.src[c];
 }
 
-// Bounded grid barrier for the cooperative Jacobi kernel: after ~2^24 polls
-// it records DERR_TIMEOUT and returns false.
-__device__ bool darcy_barrier(JacobiSync *js, DarcyCtl *ctl, unsigned nblocks)
+// Bounded wait of thread 0 until *p >= target; false (and DERR_TIMEOUT in
+// the engine's error flag) after ~2^22 polls, or as soon as another block
+// has flagged an error.
+__device__ __forceinline__ bool jacobi_wait_ge(const unsigned *p, unsigned target, DarcyCtl *ctl)
 {
-    __syncthreads();
-    __shared__ int ok;
-    if (threadIdx.x == 0) {
-        volatile unsigned *gen = &js->gen;
-        const unsigned g = *gen;
-        __threadfence();
-        bool last;
-        if (nblocks > 64) {
-            const unsigned s = blockIdx.x % 16u, members = (nblocks - s + 15u) / 16u;
-            last = false;
-            if (atomicAdd(&js->sub[s][0], 1u) == members - 1u) {
-                js->sub[s][0] = 0;
-                __threadfence();
-                last = atomicAdd(&js->count, 1u) == 15u;
-            }
-        } else {
-            last = atomicAdd(&js->count, 1u) == nblocks - 1u;
+    unsigned spins = 0, nap = 16;
+    for (;;) {
+        unsigned v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        if (v >= target) return true;
+        if (++spins > (1u << 22)) {
+            atomicCAS(&ctl->err, 0, DERR_TIMEOUT);
+            return false;
         }
-        ok = 1;
-        if (last) {
-            js->count = 0;
-            __threadfence();
-            atomicAdd(&js->gen, 1u);
-        } else {
-            unsigned spins = 0, nap = 32;
-            while (*gen == g) {
-                if (++spins > (1u << 24)) {
-                    atomicCAS(&ctl->err, 0, DERR_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-                if (((volatile int *)&ctl->err)[0] == DERR_TIMEOUT) { ok = 0; break; }
-                __nanosleep(nap);
-                if (nap < 256) nap <<= 1;
-            }
-        }
-        __threadfence();
+        if (*(volatile int *)&ctl->err != 0) return false;
+        __nanosleep(nap);
+        if (nap < 128) nap <<= 1;
     }
-    __syncthreads();
-    return ok != 0;
+}
+
+__device__ __forceinline__ bool jacobi_is_check(unsigned it, unsigned maxiter, int exact_stop)
+{
+    return exact_stop || it % 10u == 0u || it + 1u == maxiter;
 }
 
 // The Jacobi iterations of the reference (device.cu:2184-2386):
 // p_new = p_old + 0.5 dp_expl + 0.5 dp_impl(p); p_new <- 0.95 p + 0.05 p_new;
 // residual (p_new - p)/(p + 1e-16); stop when the maximum |residual| is at
-// most the tolerance at an iteration divisible by 10.
+// most the tolerance at an iteration divisible by 10 (every iteration with
+// exact_stop).
+//
+// Block b updates the cells [b*chunk, (b+1)*chunk).  Before iteration i it
+// waits until the blocks whose cells lie within reach (one z layer, one row
+// and one cell: the stencil and the periodic ghost faces the cells write)
+// have completed iteration i-1, which makes their part of iterate i-1
+// visible and frees the buffer iteration i overwrites.  The stop decision of
+// a check iteration c needs every block's residual; it is taken at the start
+// of iteration c+2, so iteration c+1 is computed while the last blocks
+// arrive (iteration c+1 writes the other buffer: iterate c stays intact and
+// is the result if the solve stops at c).
 __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, JacobiCoef C, double *pa,
                                                 double *pb, DarcyCtl *ctl, JacobiSync *js, int exact_stop)
 {
     __shared__ double wmax[8];
-    const unsigned G = gridDim.x;
+    __shared__ int s_state;          // 0 continue, 1 stop, 2 abort
+    __shared__ long long s_final;    // iterate the solve ends with
+    __shared__ long long s_conv_at;
+    const unsigned G = gridDim.x, b = blockIdx.x;
     const unsigned n = (unsigned)D.nx * D.ny * D.nz;
-    const unsigned stride = G * blockDim.x;
-    double *cur = pa, *nxt = pb;
-    long long nijac_done = 0;
-    long long converged_at = -1;
-    bool stop = false, conv = false;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ctl->res_bits[0] = 0ull;
-        ctl->res_bits[1] = 0ull;
-        ctl->res_bits[2] = 0ull;
+    const unsigned maxiter = D.maxiter;
+    const unsigned chunk = (n + G - 1) / G;
+    const unsigned lo = min(n, b * chunk), hi = min(n, lo + chunk);
+    const unsigned reach = (unsigned)D.nx * D.ny + (unsigned)D.nx + 1u;
+    const unsigned nb_lo = lo > reach ? (lo - reach) / chunk : 0u;
+    const unsigned nb_hi = min(G - 1u, (hi + reach) / chunk);
+    // thread 0's view of the decisions
+    unsigned next_dec = 0, dec_count = 0, scanned = 0;
+    if (threadIdx.x == 0) {
+        s_state = 0;
+        s_final = -1;
+        s_conv_at = -1;
     }
-    if (!darcy_barrier(js, ctl, G)) return;
-    for (unsigned nijac = 0; nijac < D.maxiter && !stop; ++nijac) {
+    __syncthreads();
+
+    // Decides check iteration c (thread 0): waits for every block's arrival,
+    // scans the residual maxima up to c, sets s_state / s_final.
+    auto decide = [&](unsigned c) {
+        const unsigned k = dec_count;
+        if (!jacobi_wait_ge(&js->arrive[k % kJacobiChecks][0], G, ctl)) {
+            s_state = 2;
+            return;
+        }
+        __threadfence();
+        bool nan = false;
+        double mc = 0.0;
+        for (unsigned j = scanned; j <= c; ++j) {
+            const unsigned long long bits = __ldcg(&js->ring[j % kJacobiRing]);
+            if (bits == ~0ull) { nan = true; break; }
+            const double m = __longlong_as_double((long long)bits);
+            if (m <= D.tolerance && s_conv_at < 0) s_conv_at = j;
+            if (j == c) mc = m;
+        }
+        scanned = c + 1;
+        // every block has waited on the counter of the check decided two
+        // decisions ago (it arrived here after deciding it)
+        if (b == 0 && k >= 2) js->arrive[(k - 2) % kJacobiChecks][0] = 0u;
+        if (nan) {
+            atomicCAS(&ctl->err, 0, DERR_NAN);
+            s_state = 2;
+            s_final = c;
+        } else if (mc <= D.tolerance && (exact_stop || c % 10u == 0u)) {
+            s_state = 1;
+            s_final = c;
+        }
+        ++dec_count;
+        // the next check iteration
+        unsigned nx = c + 1;
+        while (nx < maxiter && !jacobi_is_check(nx, maxiter, exact_stop)) ++nx;
+        next_dec = nx;
+    };
+
+    unsigned it = 0;
+    for (; it < maxiter; ++it) {
+        if (threadIdx.x < 32) {
+            if (threadIdx.x == 0)
+                while (s_state == 0 && next_dec < maxiter && next_dec + 2u <= it) decide(next_dec);
+            __syncwarp();
+            if (s_state == 0 && it > 0) {
+                // the lanes of warp 0 watch the neighbours in parallel
+                bool ok = true;
+                for (unsigned q = nb_lo + threadIdx.x; q <= nb_hi; q += 32)
+                    if (q != b && !jacobi_wait_ge(&js->done[q][0], it, ctl)) ok = false;
+                if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0) s_state = 2;
+                __threadfence();
+            }
+        }
+        __syncthreads();
+        if (s_state != 0) break;
+        const bool even = (it & 1u) == 0u;
+        const double *cur = even ? pa : pb;
+        double *nxt = even ? pb : pa;
         double lmax = 0.0;
         bool nan = false;
-        for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        for (unsigned i = lo + threadIdx.x; i < hi; i += blockDim.x) {
             const int x = (int)(i % D.nx), y = (int)((i / D.nx) % D.ny),
                       z = (int)(i / ((unsigned)D.nx * D.ny));
             const unsigned c = didx(D, x, y, z);
@@ -623,40 +682,43 @@ __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, Ja
             ghost_from<1>(D, nxt, x, y, z, &p_new);
             if (D.bc_bot == 4 || D.bc_top == 4) flux_ghost_next(D, F.k, nxt, x, y, z, p);
         }
-        // maximum over the grid: warp, block, then one atomic per block
+        // block maximum, one atomic per block into this iteration's slot
         for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
         if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = lmax;
-        __syncthreads();
+        const bool any_nan = __syncthreads_or(nan);
         if (threadIdx.x == 0) {
             double bm = 0.0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) bm = fmax(bm, wmax[w]);
-            atomicMax(&ctl->res_bits[nijac % 3], (unsigned long long)__double_as_longlong(bm));
+            unsigned long long *slot = &js->ring[it % kJacobiRing];
+            if (any_nan) atomicExch(slot, ~0ull);
+            else atomicMax(slot, (unsigned long long)__double_as_longlong(bm));
+            // the slot of iteration it + kJacobiRing / 2 was last used by
+            // iteration it - kJacobiRing / 2, scanned by every block long ago
+            if (b == 0) js->ring[(it + kJacobiRing / 2) % kJacobiRing] = 0ull;
+            __threadfence();
+            asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(&js->done[b][0]), "r"(it + 1u) : "memory");
+            if (jacobi_is_check(it, maxiter, exact_stop)) {
+                unsigned k = 0;   // index of this check among the checks
+                // checks before `it`: iterations 0, 10, 20, ... (every
+                // iteration with exact_stop), plus maxiter - 1
+                k = exact_stop ? it : it / 10u + ((it % 10u) ? 1u : 0u);
+                atomicAdd(&js->arrive[k % kJacobiChecks][0], 1u);
+            }
         }
-        if (__syncthreads_or(nan) && threadIdx.x == 0) atomicExch(&ctl->res_bits[nijac % 3], ~0ull);
-        if (!darcy_barrier(js, ctl, G)) return;
-        const unsigned long long bits = ((volatile unsigned long long *)ctl->res_bits)[nijac % 3];
-        // slot (nijac + 2) % 3 was last read before this barrier and is next
-        // written after the following one
-        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->res_bits[(nijac + 2) % 3] = 0ull;
-        nijac_done = nijac;
-        if (bits == ~0ull) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&ctl->err, 0, DERR_NAN);
-            stop = true;
-        } else {
-            const double m = __longlong_as_double((long long)bits);
-            if (m <= D.tolerance && converged_at < 0) converged_at = nijac;
-            if (m <= D.tolerance && (exact_stop || nijac % 10 == 0)) stop = conv = true;
-        }
-        double *t = cur;
-        cur = nxt;
-        nxt = t;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ctl->nijac_last = nijac_done;
-        ctl->nijac_total += nijac_done + 1;
-        ctl->converged_at = converged_at;
-        ctl->converged = conv ? 1 : 0;
-        ctl->final_buf = cur == pa ? 0 : 1;
+    // decide the checks still open (the last one or two iterations)
+    if (threadIdx.x == 0) {
+        while (s_state == 0 && next_dec < it) decide(next_dec);
+    }
+    __syncthreads();
+    if (b == 0 && threadIdx.x == 0) {
+        if (s_state == 2 && s_final < 0) return;      // timeout: ctl->err is set
+        long long fin = s_final >= 0 ? s_final : (maxiter > 0 ? (long long)maxiter - 1 : 0);
+        ctl->nijac_last = fin;
+        ctl->nijac_total += fin + 1;
+        ctl->converged_at = s_conv_at;
+        ctl->converged = s_state == 1 ? 1 : 0;
+        ctl->final_buf = maxiter == 0 ? 0 : ((fin & 1) == 0 ? 1 : 0);
     }
 }
 
@@ -823,13 +885,16 @@ int Engine::darcy_init()
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi, 256, 0);
     if (per_sm < 1) return fail(ST_CUDA, "Jacobi kernel cannot be resident");
-    // resident blocks per SM of the Jacobi launch (two by default; the
-    // variable SPHB_JACOBI_BLOCKS_PER_SM overrides it for tuning runs)
-    int bps = 2;
+    // resident blocks per SM of the Jacobi launch (four by default: about
+    // one cell per thread on the 40 x 40 x 80 benchmark grid, measured
+    // fastest among 1..4; the variable SPHB_JACOBI_BLOCKS_PER_SM overrides
+    // it for tuning runs)
+    int bps = 4;
     if (const char *env = std::getenv("SPHB_JACOBI_BLOCKS_PER_SM")) bps = std::max(1, std::atoi(env));
     jacobi_grid = sms * (per_sm < bps ? per_sm : bps);
     unsigned need = cells_blocks(D);
     if ((unsigned)jacobi_grid > need) jacobi_grid = (int)need;
+    if ((unsigned)jacobi_grid > kJacobiMaxBlocks) jacobi_grid = (int)kJacobiMaxBlocks;
     if (warm_start) {
         Dd.freec = dalloc<unsigned char>(nx * ny * nz);
         Dd.guess = dalloc<double>(ng);
@@ -921,6 +986,7 @@ cudaError_t Engine::enqueue_fluid()
     // the second buffer starts as a copy (its ghost faces are read too)
     if ((e = cudaMemcpyAsync(Dd.p2, Dd.p, Dd.ng * 8, cudaMemcpyDeviceToDevice, stream)) != cudaSuccess)
         return e;
+    if ((e = cudaMemsetAsync(Dd.jsync, 0, sizeof(JacobiSync), stream)) != cudaSuccess) return e;
     int exact = darcy_exact_stop;
     JacobiCoef C{Dd.cf, Dd.ca, Dd.csrc, Dd.cbase, Dd.cfixed, (unsigned long long)Dd.ng};
     void *args[] = {(void *)&D, (void *)&F, (void *)&C, (void *)&Dd.p, (void *)&Dd.p2, (void *)&Dd.ctl,

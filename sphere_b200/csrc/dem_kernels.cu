@@ -193,7 +193,13 @@ __global__ void __launch_bounds__(256) k_tau_partials(DevParams P, DevState S)
 // last adds the partials in block order, moves the walls and advances the
 // loop counters (device.cu:2543-2545).  Launched with the reference's
 // ceil(np / 256) blocks (one block when np == 0).
-__global__ void __launch_bounds__(256) k_integrate(DevParams P, DevState S)
+// Resident 256-thread blocks per SM of the integration kernel: 3 caps it at
+// 80 registers, so 1e5 particles integrate in one wave (measured 68 -> 61 us
+// per shear step against the uncapped 102 registers and two waves).
+#ifndef SPHB_INTEGRATE_MINB
+#define SPHB_INTEGRATE_MINB 3
+#endif
+__global__ void __launch_bounds__(256, SPHB_INTEGRATE_MINB) k_integrate(DevParams P, DevState S)
 {
     __shared__ double cache[256];
     __shared__ bool last;
