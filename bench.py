@@ -224,12 +224,14 @@ def run_gpu(args):
     contacts_bytes = n * bytes_per_particle
     achieved = contacts_bytes / (prof.contacts_ms * 1e-3) / 1e9
     # launches of this library's kernels in the timed region: per DEM step
-    # k_resort, k_nl_build, k_contacts, k_integrate (+2 for the shear-stress
-    # wall) on the per-stage path; one k_persistent per call on the fused path
+    # k_resort (with the list rebuild), k_contacts, k_integrate (+2 for the
+    # shear-stress wall, +2 with bonds) on the per-stage path; one
+    # k_persistent per call on the fused path
     if info.step_path == 1:
         timed_launches = args.steps
     else:
-        timed_launches = (4 + (2 if d.nw > 0 and d.wmode[0] == 3 else 0)) * INTERVAL * args.steps
+        per_step = 3 + (2 if d.nw > 0 and d.wmode[0] == 3 else 0) + (2 if d.nb0 > 0 else 0)
+        timed_launches = per_step * INTERVAL * args.steps
     out = {
         "metric": "particle-steps/s",
         "value": value,
@@ -282,6 +284,8 @@ def run_gpu(args):
         out["darcy"] = darcy_leg(args)
     if args.batch_boxes > 0:
         out["batch"] = batch_leg(args)
+    if args.large_particles > 0:
+        out["large"] = large_leg(args)
     return out
 
 
@@ -359,6 +363,55 @@ def batch_leg(args):
         "ms_per_step": 1e3 * step_s / len(times), "dem_steps_per_step": interval,
         "launch": cfg, "autotuner_trials": len(trials),
         "best_trial_ms_per_step": min(t["ms_per_step"] for t in trials) if trials else None,
+    }
+
+
+def large_leg(args):
+    """The large polydisperse cohesive packing (4e6 spheres, log-normal
+    radii, bonded initial neighbours), mixed precision, per-stage kernels:
+    particle-steps/s, and the DRAM-roofline fraction of the sort and of the
+    contact stage (algorithmic bytes per particle: hash 32 + sort 16 +
+    reorder 180 = 228 per sort; contacts 184 + 56 Z per step)."""
+    from sphere_b200 import configs
+    from sphere_b200.engine import Engine
+    d = configs.large_cohesive_packing(n=args.large_particles, seed=SEED + 3)
+    n, nb0 = d.np, d.nb0
+    interval = 20
+    with Engine(d, precision="mixed", graph_steps=interval) as eng:
+        eng.step(2 * interval)
+        times = [eng.step_timed(interval) for _ in range(args.large_steps)]
+        prof = eng.profile(5)
+        sort_ms = eng.time_sort(3)
+        zbar = mean_contacts(eng, n)
+        info = eng.info()
+    # the plain FP64 drop-in (faithful arithmetic) on the same packing
+    with Engine(d, precision="faithful", graph_steps=interval) as eng:
+        eng.step(2 * interval)
+        times_fp64 = [eng.step_timed(interval) for _ in range(args.large_steps)]
+    fp64_rate = n * interval * len(times_fp64) / (float(numpy.sum(times_fp64)) * 1e-3)
+    peak, peak_kind = load_peaks()
+    step_s = float(numpy.sum(times)) * 1e-3
+    contacts_bpp = 184.0 + 56.0 * zbar
+    contacts_gbs = n * contacts_bpp / (prof.contacts_ms * 1e-3) / 1e9
+    sort_gbs = n * 228.0 / (sort_ms * 1e-3) / 1e9
+    return {
+        "workload": f"large cohesive packing, N={n}, log-normal radii (median 0.01 m, sigma_ln 0.3, "
+                    f"clipped to [0.004, 0.03] m), {nb0} bonds (k 1e7, tensile strength 1e5 Pa), "
+                    "E=7e8 Pa, mu=0.5, periodic x/y, bottom wall, gravity, mixed precision",
+        "particle_steps_per_s": n * interval * len(times) / step_s,
+        "ms_per_dem_step": 1e3 * step_s / (interval * len(times)),
+        "fp64_plain_particle_steps_per_s": fp64_rate,
+        "mixed_over_fp64": n * interval * len(times) / step_s / fp64_rate,
+        "mean_contacts_per_particle": zbar,
+        "step_path": "persistent" if info.step_path == 1 else "per-stage",
+        "stage_ms_per_dem_step": {"resort": prof.resort_ms, "contacts": prof.contacts_ms,
+                                  "bonds": prof.bonds_ms, "integrate": prof.integrate_ms,
+                                  "step": prof.step_ms},
+        "sort": {"ms": sort_ms, "algorithmic_bytes_per_particle": 228.0, "achieved_gbs": sort_gbs,
+                 "frac": sort_gbs / peak},
+        "contacts": {"algorithmic_bytes_per_particle": contacts_bpp, "achieved_gbs": contacts_gbs,
+                     "frac": contacts_gbs / peak},
+        "peak_gbs": peak, "peak_source": peak_kind,
     }
 
 
@@ -443,8 +496,12 @@ def main():
     ap.add_argument("--batch-boxes", type=int, default=256,
                     help="boxes of the batched-ensemble leg (0 skips it)")
     ap.add_argument("--batch-steps", type=int, default=5)
-    ap.add_argument("--legs", default="shear,darcy,batch",
-                    help="comma list of legs to run: shear (the headline), darcy, batch")
+    ap.add_argument("--large-particles", type=int, default=4_000_000,
+                    help="spheres of the large cohesive-packing leg (0 skips it)")
+    ap.add_argument("--large-steps", type=int, default=5,
+                    help="timed calls of 20 DEM steps in the large leg")
+    ap.add_argument("--legs", default="shear,darcy,batch,large",
+                    help="comma list of legs to run: shear (the headline), darcy, batch, large")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -465,12 +522,16 @@ def main():
             out["darcy"] = darcy_leg(args)
         if "batch" in legs and args.batch_boxes > 0:
             out["batch"] = batch_leg(args)
+        if "large" in legs and args.large_particles > 0:
+            out["large"] = large_leg(args)
         print(json.dumps(out), flush=True)
         return 0
     if "darcy" not in legs:
         args.darcy_steps = 0
     if "batch" not in legs:
         args.batch_boxes = 0
+    if "large" not in legs:
+        args.large_particles = 0
     print(json.dumps(run_gpu(args)), flush=True)
     return 0
 

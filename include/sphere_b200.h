@@ -182,6 +182,12 @@ int sph_write_bin(sph_engine *e, const char *path);
 
 int sph_get_info(sph_engine *e, sph_info *info);
 
+/* Device time of the cell hash + stable cell sort + reorder of the current
+ * state (the reference's calcParticleCellID + sort_by_key + reorderArrays,
+ * src/device.cu:1066-1114), averaged over reps forced sorts.  A sort of
+ * sorted particles is the identity, so the run is unchanged. */
+int sph_time_sort(sph_engine *e, int reps, double *ms_per_sort);
+
 /* Energy sum of the current state, computed on the device.  Replaces
  * sim.energy(method) (python/sphere.py:4311-4380); method is one of "pot",
  * "kin", "rot", "shear", "shearrate", "visc_n", "visc_n_rate", "bondpot"

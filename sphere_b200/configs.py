@@ -13,6 +13,10 @@ Workloads (the sizes of the published benchmark configurations):
 * :func:`shear_benchmark` -- a settled packing under a top wall at normal
   stress sigma0 with the top layer sheared along x (N = 100,000, radii
   U(0.008, 0.012) m, Young's modulus contact E = 7e8 Pa, mu = 0.5).
+* :func:`large_cohesive_packing` -- N spheres with log-normal radii bonded
+  to their initial neighbours (N = 4,000,000, median radius 0.01 m, sigma_ln
+  0.3, clipped to [0.004, 0.03] m, bonds within 1.05 x the radius sum,
+  bond stiffness 1e7, tensile strength 1e5 Pa, E = 7e8 Pa, mu = 0.5).
 * :func:`two_particle` / :func:`wall_particle` -- the reference's collision
   test set-ups (``tests/contactmodel.py``, ``tests/contactmodel_wall.py``).
 """
@@ -488,3 +492,107 @@ def batch_shear_boxes(nbox: int = 256, seed: int = 7, n_min: int = 2000, n_max: 
         boxes.append(fcc_shear_box(n, seed * 100003 + b, sigma0=sigma0, shear_velocity=vs, mu=mu))
         meta.append({"n": n, "sigma0": sigma0, "shear_velocity": vs, "mu": mu})
     return boxes, meta
+
+
+def large_cohesive_packing(n: int = 4_000_000, seed: int = 4, layers=None,
+                           r_median: float = 0.01, sigma_ln: float = 0.3,
+                           r_lo: float = 0.004, r_hi: float = 0.03,
+                           bond_factor: float = 1.05, v_max: float = 0.01) -> BinData:
+    """The large polydisperse cohesive packing: n spheres with radii
+    exp(N(ln r_median, sigma_ln)) clipped to [r_lo, r_hi], periodic x/y,
+    the bottom wall at z = 0, gravity, Young's-modulus contact E = 7e8 Pa,
+    mu = 0.5, and parallel bonds (stiffness k_n = k_t = 1e7, tensile
+    strength 1e5 Pa, no shear limit, lambda_bar = 1) between every pair of
+    initial neighbours closer than bond_factor x the radius sum.
+
+    The start is dense without a settling run: radii are sorted (largest at
+    the bottom) and placed in horizontal square lattices, one per layer,
+    whose spacing W / cols is the smallest at or above the layer's largest
+    diameter, so in-layer neighbours touch or nearly touch; each layer rests
+    on the one below at the sum of the two layers' largest radii.  Nothing
+    overlaps initially.  Bonds join in-layer lattice neighbours and the
+    nearest sites of adjacent layers when they satisfy the distance
+    criterion; pairs across the periodic faces are left unbonded (the bond
+    law measures the direct distance).  Initial velocities are uniform in
+    [-v_max, v_max] per axis (as in the settling lattice), so contacts form
+    and bonds strain from the first steps."""
+    rng = numpy.random.default_rng(seed)
+    r = numpy.exp(rng.normal(math.log(r_median), sigma_ln, n)).clip(r_lo, r_hi)
+    r = numpy.sort(r)[::-1].copy()
+    if layers is None:
+        # 150 layers at 4e6 spheres; smaller cuts keep the aspect ratio
+        layers = max(3, int(round(150 * (n / 4.0e6) ** (1.0 / 3.0))))
+    W = 2.0 * r_median * math.ceil(math.sqrt(n / layers))
+    x = numpy.empty((n, 3))
+    lay = []                                  # (start, count, cols, spacing, z)
+    idx, z_prev, r_prev = 0, 0.0, 0.0
+    while idx < n:
+        rmax = float(r[idx])
+        cols = max(3, int(W // (2.0 * rmax)))
+        sp = W / cols
+        cnt = min(cols * cols, n - idx)
+        zc = rmax if not lay else z_prev + r_prev + rmax + 1e-7
+        i = numpy.arange(cnt)
+        x[idx:idx + cnt, 0] = (i % cols + 0.5) * sp
+        x[idx:idx + cnt, 1] = (i // cols + 0.5) * sp
+        x[idx:idx + cnt, 2] = zc
+        lay.append((idx, cnt, cols, sp, zc))
+        idx += cnt
+        z_prev, r_prev = zc, rmax
+    pairs = []
+    for li, (st, cnt, cols, sp, zc) in enumerate(lay):
+        i = numpy.arange(cnt)
+        ix, iy = i % cols, i // cols
+        for di, ok in ((1, ix + 1 < cols), (cols, iy + 1 < cols)):
+            a = i[ok & (i + di < cnt)]
+            b = a + di
+            keep = sp < bond_factor * (r[st + a] + r[st + b])
+            pairs.append(numpy.column_stack([st + a[keep], st + b[keep]]))
+        if li == 0:
+            continue
+        # nearest sites of the layer below
+        st0, cnt0, cols0, sp0, z0 = lay[li - 1]
+        px, py = x[st:st + cnt, 0], x[st:st + cnt, 1]
+        fx = numpy.floor(px / sp0 - 0.5).astype(numpy.int64)
+        fy = numpy.floor(py / sp0 - 0.5).astype(numpy.int64)
+        for ox in (0, 1):
+            for oy in (0, 1):
+                jx, jy = fx + ox, fy + oy
+                j = jy * cols0 + jx
+                ok = (jx >= 0) & (jx < cols0) & (jy >= 0) & (jy < cols0) & (j < cnt0)
+                a = numpy.nonzero(ok)[0]
+                jj = st0 + j[a]
+                ii = st + a
+                dist = numpy.sqrt(((x[ii] - x[jj]) ** 2).sum(axis=1))
+                keep = dist < bond_factor * (r[ii] + r[jj])
+                pairs.append(numpy.column_stack([jj[keep], ii[keep]]))
+    bonds = numpy.concatenate(pairs).astype(numpy.uint32) if pairs else numpy.zeros((0, 2), numpy.uint32)
+
+    d = BinData()
+    _particles(d, n)
+    d.x = x
+    d.radius = r
+    d.vel = rng.uniform(-v_max, v_max, size=(n, 3))
+    default_params(d, mu_s=0.5, mu_d=0.5, k_n=1e7, k_t=1e7)
+    d.E = 7e8
+    d.g = numpy.array([0.0, 0.0, -9.81])
+    cell = 2.1 * r_hi if r.max() <= r_hi else 2.1 * float(r.max())
+    ncell = max(3, int(math.floor(W / cell)))
+    top = float(numpy.max(x[:, 2] + r))
+    nz = max(3, int(math.ceil(top * 1.1 / (W / ncell))))
+    grid_for(d, L=[W, W, nz * (W / ncell)], dx=W / ncell)
+    d.periodic = 1
+    d.nw = 0
+    d.nb0 = len(bonds)
+    d.bonds = bonds
+    d.bonds_delta_n = numpy.zeros(d.nb0)
+    d.bonds_delta_t = numpy.zeros((d.nb0, 3))
+    d.bonds_omega_n = numpy.zeros(d.nb0)
+    d.bonds_omega_t = numpy.zeros((d.nb0, 3))
+    d.lambda_bar = 1.0
+    d.sigma_b = 1e5
+    d.tau_b = numpy.inf
+    init_temporal(d, total=1.0, file_dt=1.0)
+    d.time_total = 5000 * d.time_dt
+    d.time_file_dt = d.time_total
+    return d

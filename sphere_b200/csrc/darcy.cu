@@ -606,11 +606,11 @@ __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, Ja
     // scans the residual maxima up to c, sets s_state / s_final.
     auto decide = [&](unsigned c) {
         const unsigned k = dec_count;
+        // acquire: every block's residual (ordered before its release-add)
         if (!jacobi_wait_ge(&js->arrive[k % kJacobiChecks][0], G, ctl)) {
             s_state = 2;
             return;
         }
-        __threadfence();
         bool nan = false;
         double mc = 0.0;
         for (unsigned j = scanned; j <= c; ++j) {
@@ -651,9 +651,10 @@ __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, Ja
                 for (unsigned q = nb_lo + threadIdx.x; q <= nb_hi; q += 32)
                     if (q != b && !jacobi_wait_ge(&js->done[q][0], it, ctl)) ok = false;
                 if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0) s_state = 2;
-                __threadfence();
             }
         }
+        // the acquire loads above and this barrier make the neighbours'
+        // cells visible to the whole block
         __syncthreads();
         if (s_state != 0) break;
         const bool even = (it & 1u) == 0u;
@@ -685,8 +686,11 @@ __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, Ja
         // block maximum, one atomic per block into this iteration's slot
         for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
         if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = lmax;
+        // the barrier orders every thread's cell stores before thread 0's
+        // release (cumulative at GPU scope), so the neighbours may go on
         const bool any_nan = __syncthreads_or(nan);
         if (threadIdx.x == 0) {
+            asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(&js->done[b][0]), "r"(it + 1u) : "memory");
             double bm = 0.0;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) bm = fmax(bm, wmax[w]);
             unsigned long long *slot = &js->ring[it % kJacobiRing];
@@ -695,14 +699,13 @@ __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, Ja
             // the slot of iteration it + kJacobiRing / 2 was last used by
             // iteration it - kJacobiRing / 2, scanned by every block long ago
             if (b == 0) js->ring[(it + kJacobiRing / 2) % kJacobiRing] = 0ull;
-            __threadfence();
-            asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(&js->done[b][0]), "r"(it + 1u) : "memory");
             if (jacobi_is_check(it, maxiter, exact_stop)) {
-                unsigned k = 0;   // index of this check among the checks
-                // checks before `it`: iterations 0, 10, 20, ... (every
-                // iteration with exact_stop), plus maxiter - 1
-                k = exact_stop ? it : it / 10u + ((it % 10u) ? 1u : 0u);
-                atomicAdd(&js->arrive[k % kJacobiChecks][0], 1u);
+                // index of this check among the checks: iterations 0, 10,
+                // 20, ... (every iteration with exact_stop), plus maxiter - 1;
+                // the release orders the residual above before the arrival
+                const unsigned k = exact_stop ? it : it / 10u + ((it % 10u) ? 1u : 0u);
+                asm volatile("red.release.gpu.global.add.u32 [%0], 1;"
+                             :: "l"(&js->arrive[k % kJacobiChecks][0]) : "memory");
             }
         }
     }

@@ -614,7 +614,7 @@ __global__ void __launch_bounds__(128, SPHB_CONTACT_MINB) k_contacts(DevParams P
 {
     extern __shared__ uint32_t srow[];   // blockDim * nc slot partners
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k == 0 && S.ctl->nl_rebuild) S.ctl->nl_rebuild = 0;  // k_nl_build has run
+    if (k == 0 && S.ctl->nl_rebuild) S.ctl->nl_rebuild = 0;  // k_resort has rebuilt the lists
     if (S.ctl->err || k >= P.np) return;
     ContactOut c;
     if (!contact_particle<PREC, MODEL>(P, S, k, srow, blockDim.x, threadIdx.x, c)) return;

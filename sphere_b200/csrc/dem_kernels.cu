@@ -9,16 +9,6 @@
 
 namespace sphb {
 
-// Neighbour-list rebuild of the per-stage path: runs every step, works
-// only when DevCtl::nl_rebuild is set (k_contacts clears it).
-__global__ void __launch_bounds__(128) k_nl_build(DevParams P, DevState S)
-{
-    unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (S.ctl->err || !S.ctl->nl_rebuild || k >= P.np) return;
-    nl_build_particle(P, S, k);
-    if (k == 0) S.ctl->nl_builds += 1;
-}
-
 // Occupancy masks of the slot rows (after the rows were set from the host).
 __global__ void k_occ_from_rows(DevParams P, DevState S)
 {
@@ -256,19 +246,10 @@ __global__ void k_hash(DevParams P, DevState S)
 // ---------------------------------------------------------------------
 static inline unsigned blocks_for(unsigned n, unsigned b) { return (n + b - 1) / b; }
 
-cudaError_t launch_nl_build(const DevParams &P, const DevState &S, cudaStream_t st)
-{
-    if (P.np == 0) return cudaSuccess;
-    k_nl_build<<<blocks_for(P.np, 128), 128, 0, st>>>(P, S);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cudaStream_t st)
 {
     if (P.np == 0) return cudaSuccess;
     const unsigned B = 128;
-    cudaError_t e = launch_nl_build(P, S, st);
-    if (e != cudaSuccess) return e;
     dim3 grid(blocks_for(P.np, B));
     if (P.contactmodel == 2) {
         size_t smem = (size_t)B * P.nc * sizeof(uint32_t);

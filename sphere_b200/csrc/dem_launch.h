@@ -12,8 +12,6 @@ namespace sphb {
 cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cudaStream_t st);
 // mixed precision: FP64 overlaps, FP32 contact laws, FP64 accumulation
 cudaError_t launch_contacts_mixed(const DevParams &P, const DevState &S, cudaStream_t st);
-// neighbour-list rebuild (a no-op unless DevCtl::nl_rebuild)
-cudaError_t launch_nl_build(const DevParams &P, const DevState &S, cudaStream_t st);
 cudaError_t launch_bonds(const DevParams &P, const DevState &S, int prec, double4 *bond_f,
                          double4 *bond_t, cudaStream_t st);
 // shear-stress reduction (wmode 3), then one kernel: integration, wall
@@ -21,9 +19,11 @@ cudaError_t launch_bonds(const DevParams &P, const DevState &S, int prec, double
 cudaError_t launch_integrate(const DevParams &P, const DevState &S, cudaStream_t st);
 cudaError_t launch_occ_from_rows(const DevParams &P, const DevState &S, cudaStream_t st);
 cudaError_t launch_hash(const DevParams &P, const DevState &S, cudaStream_t st);
-// force = 1 sorts unconditionally; otherwise only when DevCtl::resort is set
+// force = 1 sorts unconditionally; otherwise only when DevCtl::resort is
+// set.  with_nl = 1 also rebuilds the neighbour lists in the same launch
+// when they are stale (DevCtl::nl_rebuild) or the sort ran.
 cudaError_t launch_resort(const DevParams &P, const DevState &S, unsigned char *scratch,
-                          int force, cudaStream_t st);
+                          int force, cudaStream_t st, int with_nl = 0);
 size_t resort_scratch_bytes(size_t np);
 
 // Gathers sorted storage into original order: dst[orig_of[k]] = src[k].

@@ -11,8 +11,6 @@ cudaError_t launch_contacts_mixed(const DevParams &P, const DevState &S, cudaStr
 {
     if (P.np == 0) return cudaSuccess;
     const unsigned B = 128;
-    cudaError_t e = launch_nl_build(P, S, st);
-    if (e != cudaSuccess) return e;
     dim3 grid((P.np + B - 1) / B);
     if (P.contactmodel == 2) {
         size_t smem = (size_t)B * P.nc * sizeof(uint32_t);

@@ -168,8 +168,7 @@ int Engine::allocate_and_upload()
     bond_f = dalloc<double4>(h.nb0);
     bond_t = dalloc<double4>(h.nb0);
     tmp = dalloc<unsigned char>(std::max<size_t>(slots * 32, n * 32) + 64);
-    if (!S.x || !S.ctl || !tmp || !S.delta_t || !S.perm_scratch)
-        return fail(ST_CUDA, "device allocation failed");
+    if (alloc_failed) return fail(ST_CUDA, "device allocation failed");
 
     // bonds: CSR of (bond << 1 | side) per particle, bonds in increasing order
     std::vector<uint32_t> ptr(n + 1, 0), list;
@@ -290,7 +289,7 @@ cudaError_t Engine::enqueue_stage(int stage)
 {
     const int prec = precision == 0 ? 0 : 1;
     switch (stage) {
-    case 0: return launch_resort(P, S, S.perm_scratch, 0, stream);
+    case 0: return launch_resort(P, S, S.perm_scratch, 0, stream, 1);
     case 1:
         if (precision == SPH_PREC_MIXED) return launch_contacts_mixed(P, S, stream);
         return launch_contacts(P, S, prec, stream);
@@ -806,7 +805,9 @@ static int open_common(std::unique_ptr<Engine> &eng, const sph_opts *opts)
         e.precision != SPH_PREC_MIXED)
         return e.fail(sphb::ST_ARG, "unknown precision mode");
     if (e.hs.contactmodel == 3)
-        return e.fail(sphb::ST_UNSUPPORTED, "contact model 3 (Hertz-Mindlin) is not built");
+        return e.fail(sphb::ST_UNSUPPORTED,
+                      "contact model 3 (Hertz-Mindlin) is not built: the reference's contactHertz "
+                      "takes powers of the negative overlap and returns NaN forces for every contact");
     if (e.hs.contactmodel != 1 && e.hs.contactmodel != 2)
         return e.fail(sphb::ST_INPUT, "contact model not understood");
     int rc = sphb::check_values(e.hs, e.err);
@@ -1007,6 +1008,32 @@ int sph_get_info(sph_engine *e, sph_info *info)
     info->resorts = g.last_ctl.resorts;
     g.persist_describe(info);
     return rc;
+}
+
+int sph_time_sort(sph_engine *e, int reps, double *ms_per_sort)
+{
+    if (!e || !ms_per_sort || reps < 1) return SPH_ERR_ARG;
+    Engine &g = *e->e;
+    int rc = g.poll_errors("sort timing");
+    if (rc < 0) return rc;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, g.stream);
+    cudaError_t err = cudaSuccess;
+    for (int i = 0; i < reps && err == cudaSuccess; ++i) {
+        err = sphb::launch_hash(g.P, g.S, g.stream);
+        if (err == cudaSuccess) err = sphb::launch_resort(g.P, g.S, g.S.perm_scratch, 1, g.stream);
+    }
+    cudaEventRecord(b, g.stream);
+    cudaEventSynchronize(b);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (err != cudaSuccess) return g.cuda_fail(err, "sort timing");
+    *ms_per_sort = ms / reps;
+    return g.poll_errors("sort timing");
 }
 
 int sph_energy(sph_engine *e, const char *method, double *out)

@@ -44,6 +44,7 @@ public:
     DevState S{};
     cudaStream_t stream = nullptr;
     std::vector<void *> allocations;
+    bool alloc_failed = false;    // a dalloc() returned null
     void *host_pinned = nullptr;
     unsigned char *tmp = nullptr;
     double4 *bond_f = nullptr, *bond_t = nullptr;
@@ -142,7 +143,10 @@ template <class T> T *Engine::dalloc(size_t n)
 {
     void *p = nullptr;
     size_t bytes = n ? n * sizeof(T) : sizeof(T);
-    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        alloc_failed = true;
+        return nullptr;
+    }
     cudaMemsetAsync(p, 0, bytes, stream);
     allocations.push_back(p);
     return (T *)p;

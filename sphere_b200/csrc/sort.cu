@@ -13,6 +13,7 @@
 #include "dem_state.h"
 #include "dem_launch.h"
 #include "resort_device.cuh"
+#include "dem_device.cuh"
 
 #include <cooperative_groups.h>
 
@@ -53,25 +54,42 @@ __device__ bool grid_barrier(DevCtl *ctl, unsigned nblocks)
     return ok != 0;
 }
 
-__global__ void __launch_bounds__(256) k_resort(DevParams P, DevState S, PermScratch W, int force)
+// The pre-contact work of a step in one launch: the re-sort when a
+// particle changed cell (or `force`), then, with `with_nl`, the neighbour
+// lists when they are stale or the sort changed the indices.  Both flags
+// come from the previous step's integration, so every block reads the same
+// decision.
+__global__ void __launch_bounds__(256, 3) k_resort(DevParams P, DevState S, PermScratch W, int force,
+                                                int with_nl)
 {
     DevCtl *ctl = S.ctl;
     if (ctl->err) return;
-    if (!force && !ctl->resort) return;
+    const bool resort = force || ctl->resort;
+    const bool nl = with_nl && (resort || ctl->nl_rebuild);
+    if (!resort && !nl) return;
     auto bar = [&]() { return grid_barrier(ctl, gridDim.x); };
-    // the FP32 velocity copies of the mixed mode follow the permutation
-    if (!resort_group(P, S, W, gridDim.x, blockIdx.x, bar, true)) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ctl->resort = 0;
-        ctl->resorts += 1;
-        ctl->nl_rebuild = 1;   // sorted indices changed
+    if (resort) {
+        // the FP32 velocity copies of the mixed mode follow the permutation
+        if (!resort_group(P, S, W, gridDim.x, blockIdx.x, bar, true)) return;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            ctl->resort = 0;
+            ctl->resorts += 1;
+            ctl->nl_rebuild = 1;   // sorted indices changed (k_contacts clears it)
+        }
+        if (nl && !bar()) return;
+    }
+    if (nl) {
+        const unsigned stride = gridDim.x * blockDim.x;
+        for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < P.np; k += stride)
+            nl_build_particle(P, S, k);
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->nl_builds += 1;
     }
 }
 
 static int g_resort_grid = 0;
 
 cudaError_t launch_resort(const DevParams &P, const DevState &S, unsigned char *scratch,
-                          int force, cudaStream_t st)
+                          int force, cudaStream_t st, int with_nl)
 {
     if (P.np == 0) return cudaSuccess;
     if (g_resort_grid == 0) {
@@ -88,7 +106,7 @@ cudaError_t launch_resort(const DevParams &P, const DevState &S, unsigned char *
     if (need < grid) grid = need < 1 ? 1 : need;
     DevParams Pc = P;
     DevState Sc = S;
-    void *args[] = {(void *)&Pc, (void *)&Sc, (void *)&W, (void *)&force};
+    void *args[] = {(void *)&Pc, (void *)&Sc, (void *)&W, (void *)&force, (void *)&with_nl};
     return cudaLaunchCooperativeKernel((void *)k_resort, dim3(grid), dim3(256), args, 0, st);
 }
 

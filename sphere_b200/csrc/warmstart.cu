@@ -36,8 +36,10 @@ constexpr int kInputs = 4;       // p_prev, phi, dphi, previous pressure change
 constexpr int kTaps = 27;
 constexpr int kWElems = kTaps * kCh * kCh;   // weights per layer
 constexpr int kTile = 128;       // cells per MMA tile (M)
-constexpr size_t kConvSmem = kTaps * 4096 + kTaps * 512;
-constexpr size_t kWgradSmem = 32 * 4096 + 8 * 512;
+constexpr int kRound = 9;        // taps gathered per round of the convolution
+constexpr size_t kConvSmem = kRound * 4096 + kTaps * 512;
+constexpr int kWChunk = 64;      // cells per K chunk of the weight gradient
+constexpr size_t kWgradSmem = 16 * 4096 + 4 * 512;
 constexpr unsigned kWaitLimit = 1u << 22;
 
 using bf16 = __nv_bfloat16;
@@ -66,11 +68,17 @@ __device__ __forceinline__ bool neighbour(const ConvArgs &a, unsigned c, int tap
 
 // mode 0: out = ReLU(conv + bias) (BF16); mode 1: out channel 0 = conv +
 // bias (FP32); mode 2: out = conv * [relu_ref > 0] (BF16, no bias).
+//
+// The 27 taps go through in three rounds of 9: the block gathers a round's
+// shifted operand tiles into shared memory (36 KB), one thread issues their
+// MMAs, and the round's commit frees the tiles for the next round.  The
+// small footprint (50 KB with the weights) keeps four blocks resident per
+// SM, so one block's gathers overlap another's MMAs and epilogue.
 template <int MODE>
-__global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a)
+__global__ void __launch_bounds__(128, 4) k_conv_tc(ConvArgs a)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
-    unsigned char *sA = sm, *sB = sm + kTaps * 4096;
+    unsigned char *sA = sm, *sB = sm + kRound * 4096;
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -86,34 +94,46 @@ __global__ void __launch_bounds__(128, 1) k_conv_tc(ConvArgs a)
         uint4 v = *reinterpret_cast<const uint4 *>(a.w + ((size_t)tap * 16 + n) * 16 + h * 8);
         *reinterpret_cast<uint4 *>(sB + tap * 512 + tc::kmajor_off(n, h * 8)) = v;
     }
-    // A: the tile's neighbour values per tap, row = cell, k = channel
-    for (int i = tid; i < kTaps * 256; i += 128) {
-        const int tap = i >> 8, r = (i >> 1) & 127, h = i & 1;
-        const unsigned c = c0 + r;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        size_t nb;
-        if (c < a.ncells && neighbour(a, c, tap, nb))
-            v = *reinterpret_cast<const uint4 *>(a.in + nb * 16 + h * 8);
-        *reinterpret_cast<uint4 *>(sA + tap * 4096 + tc::kmajor_off(r, h * 8)) = v;
+    bool ok = true;
+    const uint32_t aaddr = tc::smem_u32(sA), baddr = tc::smem_u32(sB);
+    constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 16);
+    for (int round = 0; round < kTaps / kRound; ++round) {
+        // A: the tile's neighbour values per tap of this round, row = cell,
+        // k = channel
+        for (int i = tid; i < kRound * 256; i += 128) {
+            const int tl = i >> 8, r = (i >> 1) & 127, h = i & 1;
+            const int tap = round * kRound + tl;
+            const unsigned c = c0 + r;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            size_t nb;
+            if (c < a.ncells && neighbour(a, c, tap, nb))
+                v = *reinterpret_cast<const uint4 *>(a.in + nb * 16 + h * 8);
+            *reinterpret_cast<uint4 *>(sA + tl * 4096 + tc::kmajor_off(r, h * 8)) = v;
+        }
+        tc::fence_smem_to_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        const uint32_t tbase = tmem_base;
+        if (tid == 0) {
+            for (int tl = 0; tl < kRound; ++tl)
+                tc::mma_bf16(tbase, tc::sdesc(aaddr + tl * 4096, 128, 256),
+                             tc::sdesc(baddr + (round * kRound + tl) * 512, 128, 256), idesc,
+                             (round > 0 || tl > 0) ? 1u : 0u);
+            tc::mma_commit(&mbar);
+        }
+        // the round's MMAs are done before its tiles are overwritten (and
+        // before the accumulator is read)
+        if (!tc::mbar_wait_bounded(&mbar, (uint32_t)(round & 1), kWaitLimit)) {
+            if (tid == 0) atomicExch(a.err, 1);
+            (void)tc::mbar_wait_bounded(&mbar, (uint32_t)(round & 1), kWaitLimit);
+            ok = false;
+        }
+        tc::fence_after_sync();
+        __syncthreads();
+        if (!ok) break;
     }
-    tc::fence_smem_to_async();
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
     const uint32_t tbase = tmem_base;
-    if (tid == 0) {
-        const uint32_t aaddr = tc::smem_u32(sA), baddr = tc::smem_u32(sB);
-        constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 16);
-        for (int tap = 0; tap < kTaps; ++tap)
-            tc::mma_bf16(tbase, tc::sdesc(aaddr + tap * 4096, 128, 256),
-                         tc::sdesc(baddr + tap * 512, 128, 256), idesc, tap > 0 ? 1u : 0u);
-        tc::mma_commit(&mbar);
-    }
-    bool ok = tc::mbar_wait_bounded(&mbar, 0, kWaitLimit);
-    if (!ok) {
-        if (tid == 0) atomicExch(a.err, 1);
-        (void)tc::mbar_wait_bounded(&mbar, 0, kWaitLimit);   // before TMEM is released
-    }
     tc::fence_after_sync();
     uint32_t r[16];
     tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16), r);
@@ -148,20 +168,26 @@ struct WgradArgs {
     unsigned ncells;
     const bf16 *x;         // layer input [ncells][16]
     const bf16 *g;         // gradient of the layer output [ncells][16]
-    unsigned cells_per_block;  // multiple of 128
+    unsigned cells_per_block;  // multiple of kWChunk
     float *partial_w;      // [grid][512][16]: row = tap * 16 + in channel
     float *partial_b;      // [grid][16]
     int *err;
 };
 
-// Weight and bias gradients of one layer over this block's range of cells.
-__global__ void __launch_bounds__(128, 1) k_wgrad_tc(WgradArgs a)
+// Weight and bias gradients of one layer over this block's range of cells,
+// in chunks of 64 cells (K = 4 slices of 16).  A holds the shifted inputs
+// transposed, rows (tap, in channel) in four M tiles of 128, columns =
+// cells: one thread takes 8 consecutive cells of one tap, loads their 16
+// channels and writes the 16 rows' 16-byte segments (a register transpose
+// instead of 2-byte shared-memory stores).  72 KB of shared memory keep
+// three blocks resident per SM.
+__global__ void __launch_bounds__(128, 3) k_wgrad_tc(WgradArgs a)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
-    unsigned char *sA = sm, *sB = sm + 32 * 4096;
+    unsigned char *sA = sm, *sB = sm + 16 * 4096;
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base;
-    __shared__ float bsum[128][17];
+    __shared__ float bsum[kWChunk][17];
     const int tid = threadIdx.x, warp = tid >> 5;
     const unsigned cb = blockIdx.x * a.cells_per_block;
     const unsigned ce = min(cb + a.cells_per_block, a.ncells);
@@ -171,7 +197,7 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(WgradArgs a)
     }
     if (tid == 0) tc::mbar_init(&mbar, 1);
     // rows of taps 27..31 (the padding of the last M tile) stay zero
-    for (unsigned i = tid; i < 32 * 4096 / 16; i += 128)
+    for (unsigned i = tid; i < 16 * 4096 / 16; i += 128)
         reinterpret_cast<uint4 *>(sA)[i] = make_uint4(0u, 0u, 0u, 0u);
     float bacc = 0.0f;   // thread co < 16: bias gradient of channel co
     ConvArgs geo;
@@ -182,27 +208,43 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(WgradArgs a)
     const uint32_t tbase = tmem_base;
     bool ok = true;
     unsigned chunk = 0;
-    for (unsigned base = cb; base < ce; base += kTile, ++chunk) {
-        // A: tile (t, kc) holds rows (tap - 8 t) * 16 + in channel, columns = cells
-        for (int i = tid; i < kTaps * kTile; i += 128) {
-            const int tap = i >> 7, r = i & 127;
-            const unsigned c = base + r;
-            __align__(16) bf16 v[16];
-            size_t nb;
-            if (c < ce && neighbour(geo, c, tap, nb)) {
-                *reinterpret_cast<uint4 *>(&v[0]) = *reinterpret_cast<const uint4 *>(a.x + nb * 16);
-                *reinterpret_cast<uint4 *>(&v[8]) = *reinterpret_cast<const uint4 *>(a.x + nb * 16 + 8);
-            } else {
-                *reinterpret_cast<uint4 *>(&v[0]) = make_uint4(0u, 0u, 0u, 0u);
-                *reinterpret_cast<uint4 *>(&v[8]) = make_uint4(0u, 0u, 0u, 0u);
+    for (unsigned base = cb; base < ce; base += kWChunk, ++chunk) {
+        // A: item = (tap, group of 8 cells)
+        for (int item = tid; item < kTaps * (kWChunk / 8); item += 128) {
+            const int tap = item / (kWChunk / 8), g = item % (kWChunk / 8);
+            uint32_t w[8][8];   // [cell][channel pair]
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const unsigned c = base + (unsigned)(g * 8 + j);
+                size_t nb;
+                uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+                if (c < ce && neighbour(geo, c, tap, nb)) {
+                    lo = *reinterpret_cast<const uint4 *>(a.x + nb * 16);
+                    hi = *reinterpret_cast<const uint4 *>(a.x + nb * 16 + 8);
+                }
+                w[j][0] = lo.x; w[j][1] = lo.y; w[j][2] = lo.z; w[j][3] = lo.w;
+                w[j][4] = hi.x; w[j][5] = hi.y; w[j][6] = hi.z; w[j][7] = hi.w;
             }
-            unsigned char *tile = sA + ((tap >> 3) * 8 + (r >> 4)) * 4096;
-            const uint32_t row0 = (uint32_t)(tap & 7) * 16, k = (uint32_t)(r & 15);
-            for (int ci = 0; ci < 16; ++ci)
-                *reinterpret_cast<bf16 *>(tile + tc::kmajor_off(row0 + ci, k)) = v[ci];
+            unsigned char *tile = sA + ((tap >> 3) * 4 + (g >> 1)) * 4096;
+            const uint32_t kseg = (uint32_t)(g & 1) * 8;
+#pragma unroll
+            for (int cp = 0; cp < 8; ++cp) {
+                const uint32_t row = (uint32_t)(tap & 7) * 16 + 2 * cp;
+                uint4 vlo, vhi;   // channel 2cp and 2cp+1 of the 8 cells
+                vlo.x = __byte_perm(w[0][cp], w[1][cp], 0x5410);
+                vlo.y = __byte_perm(w[2][cp], w[3][cp], 0x5410);
+                vlo.z = __byte_perm(w[4][cp], w[5][cp], 0x5410);
+                vlo.w = __byte_perm(w[6][cp], w[7][cp], 0x5410);
+                vhi.x = __byte_perm(w[0][cp], w[1][cp], 0x7632);
+                vhi.y = __byte_perm(w[2][cp], w[3][cp], 0x7632);
+                vhi.z = __byte_perm(w[4][cp], w[5][cp], 0x7632);
+                vhi.w = __byte_perm(w[6][cp], w[7][cp], 0x7632);
+                *reinterpret_cast<uint4 *>(tile + tc::kmajor_off(row, kseg)) = vlo;
+                *reinterpret_cast<uint4 *>(tile + tc::kmajor_off(row + 1, kseg)) = vhi;
+            }
         }
-        // B: tile kc holds rows = output channel, columns = cells
-        {
+        // B: slice kc holds rows = output channel, columns = cells
+        if (tid < kWChunk) {
             const unsigned c = base + tid;
             __align__(16) bf16 v[16];
             if (c < ce) {
@@ -226,14 +268,14 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(WgradArgs a)
             const uint32_t aaddr = tc::smem_u32(sA), baddr = tc::smem_u32(sB);
             constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 16);
             for (int t = 0; t < 4; ++t)
-                for (int kc = 0; kc < 8; ++kc)
-                    tc::mma_bf16(tbase + (uint32_t)(t * 16), tc::sdesc(aaddr + (t * 8 + kc) * 4096, 128, 256),
+                for (int kc = 0; kc < kWChunk / 16; ++kc)
+                    tc::mma_bf16(tbase + (uint32_t)(t * 16), tc::sdesc(aaddr + (t * 4 + kc) * 4096, 128, 256),
                                  tc::sdesc(baddr + kc * 512, 128, 256), idesc,
                                  (chunk > 0 || kc > 0) ? 1u : 0u);
             tc::mma_commit(&mbar);
         }
         if (tid < 16)
-            for (int i = 0; i < 128; ++i) bacc += bsum[i][tid];
+            for (int i = 0; i < kWChunk; ++i) bacc += bsum[i][tid];
         if (!tc::mbar_wait_bounded(&mbar, chunk & 1, kWaitLimit)) {
             if (tid == 0) atomicExch(a.err, 1);
             (void)tc::mbar_wait_bounded(&mbar, chunk & 1, kWaitLimit);
@@ -649,9 +691,15 @@ WarmStart *ws_create(int nx, int ny, int nz, uint64_t seed, int train_solves)
     W->wpartial = W->alloc<float>(blocks(W->ncells, 256));
     W->sc = W->alloc<Scalars>(1);
     W->err = W->alloc<int>(1);
-    // one weight-gradient block per ~1024 cells, at least one 128-cell tile
-    W->cells_per_block = 1024;
-    W->wgrad_blocks = blocks(W->ncells, W->cells_per_block);
+    // weight-gradient blocks: three per SM, each over a multiple of 64 cells
+    {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const unsigned target = std::max(1u, std::min((unsigned)(3 * sms), blocks(W->ncells, kWChunk)));
+        W->cells_per_block = blocks(blocks(W->ncells, target), kWChunk) * kWChunk;
+        W->wgrad_blocks = blocks(W->ncells, W->cells_per_block);
+    }
     W->partial_w = W->alloc<float>((size_t)W->wgrad_blocks * 512 * 16);
     W->partial_b = W->alloc<float>((size_t)W->wgrad_blocks * 16);
     std::mt19937_64 rng(seed);

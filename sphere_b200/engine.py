@@ -117,6 +117,7 @@ def lib() -> ctypes.CDLL:
     L.sph_check_file.argtypes = [ctypes.c_char_p, ctypes.c_int]
     L.sph_check_file.restype = ctypes.c_int
     L.sph_energy.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
+    L.sph_time_sort.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.sph_porosity.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     L.sph_overlaps.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                ctypes.POINTER(ctypes.c_uint64)]
@@ -277,6 +278,12 @@ class Engine:
 
     def write_bin(self, path) -> None:
         self._check(lib().sph_write_bin(self._h, os.fsencode(path)))
+
+    def time_sort(self, reps=5) -> float:
+        """Device time in ms of one forced cell hash + sort + reorder."""
+        ms = ctypes.c_double(0.0)
+        self._check(lib().sph_time_sort(self._h, int(reps), ctypes.byref(ms)))
+        return ms.value
 
     # diagnostics of sphere's sim class, computed on the device
 

@@ -122,3 +122,26 @@ def test_darcy(tmp_path, kw):
         bad = compare_states(orc.get, ref.get, DARCY_FIELDS)
         assert not bad, bad
     assert orc.get("darcy_nijac_last")[0] > 10
+
+
+def test_reference_hertz_model_gives_nan_forces(tmp_path):
+    """contactmodel 3 in the reference (contactHertz, src/contactmodels.cuh:
+    414-591) raises the signed overlap, which is negative for every
+    contact, to the powers 3/2, 1/2 and 1/4 (powf of a negative number is
+    NaN), so its first contact turns the forces and then the positions into
+    NaN.  This is why the engine refuses model 3 (SPH_ERR_UNSUPPORTED) rather
+    than reproduce it."""
+    d = configs.two_particle(z=(2.0, 3.9), vel0=1.0)
+    d.contactmodel = 3
+    path = str(tmp_path / "hertz.bin")
+    binfile.write_bin(d, path)
+    ref = O.Reference(path)
+    ref.step(1)
+    assert numpy.all(numpy.isnan(ref.get("force")[:, :3]))
+    assert numpy.all(numpy.isnan(ref.get("x")[:, :3]))
+    # without a contact the same model leaves the particles finite
+    d.x[1, 2] = 6.0
+    binfile.write_bin(d, path)
+    ref = O.Reference(path)
+    ref.step(1)
+    assert numpy.all(numpy.isfinite(ref.get("x")[:, :3]))
