@@ -566,7 +566,7 @@ def run_distributed(args, rank, world):
     local = int(os.environ.get("LOCAL_RANK", rank))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
     n = args.particles
     d = workload(n)
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
