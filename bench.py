@@ -292,7 +292,8 @@ def run_gpu(args):
 def darcy_leg(args):
     """Darcy-coupled consolidation (40 x 40 x 80 fluid grid, residual
     tolerance 1e-8, top wall stepped 10 -> 20 -> 40 -> 80 kPa): Jacobi
-    iterations per fluid step without and with the learned warm start.  The
+    iterations per fluid step from the previous solution (the reference),
+    with the learned warm start, and with its extrapolation alone.  The
     network trains online from the first solve; the comparison uses the
     second half of the steps, exact iteration counts (the first iteration
     whose residual met the tolerance) and the reference's own count (checks
@@ -303,7 +304,8 @@ def darcy_leg(args):
     steps = args.darcy_steps
     loads = [10e3, 20e3, 40e3, 80e3]
     arms = {}
-    for warm in (False, True):
+    names = {0: "plain", 1: "warm", 2: "extrapolation"}
+    for warm in (0, 1, 2):
         eng = Engine(d, fluid=True, precision="mixed", warm_start=warm)
         mv = eng.get("walls_mvfd")
         exact, quant, ms = [], [], []
@@ -318,14 +320,14 @@ def darcy_leg(args):
         stats = eng.get("darcy_warm")
         eng.close()
         h = steps // 2
-        arms["warm" if warm else "plain"] = {
+        arms[names[warm]] = {
             "iters_exact_per_step": float(numpy.mean(exact[h:])),
             "iters_per_step": float(numpy.mean(quant[h:])),
             "ms_per_fluid_step": float(numpy.mean(ms[h:])),
             "predictions": int(stats[0]), "trained": int(stats[1]), "used_network_guess": int(stats[2]),
         }
-        log(f"darcy {'warm' if warm else 'plain'}: {arms['warm' if warm else 'plain']}")
-    p, w = arms["plain"], arms["warm"]
+        log(f"darcy {names[warm]}: {arms[names[warm]]}")
+    p, w, x = arms["plain"], arms["warm"], arms["extrapolation"]
     return {
         "workload": f"Darcy consolidation, N={d.np}, fluid grid {int(d.num[0])}x{int(d.num[1])}x{int(d.num[2])}, "
                     "mu_f=1.797e-6 Pa s, k_c=3.5e-13 m^2, beta_f=4.5e-10 1/Pa, tolerance 1e-8, "
@@ -334,7 +336,9 @@ def darcy_leg(args):
         "iters_per_step_plain": p["iters_exact_per_step"],
         "iters_per_step_warm": w["iters_exact_per_step"],
         "iteration_reduction": p["iters_exact_per_step"] / max(w["iters_exact_per_step"], 1e-9),
-        "plain": p, "warm": w,
+        "iters_per_step_extrapolation": x["iters_exact_per_step"],
+        "iteration_reduction_extrapolation_only": p["iters_exact_per_step"] / max(x["iters_exact_per_step"], 1e-9),
+        "plain": p, "warm": w, "extrapolation": x,
     }
 
 

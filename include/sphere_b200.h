@@ -53,7 +53,11 @@ typedef struct sph_opts {
     int precision;        /* SPH_PREC_* */
     int integrator;       /* 3: three-term Taylor (the reference's TY3), 2: two-term */
     int contact_capacity; /* contact slots per particle; the reference's NC is 32 */
-    int warm_start;       /* Darcy: 0 previous-step guess, 1 learned warm start */
+    int warm_start;       /* Darcy start: 0 the previous solution (the reference's),
+                             1 learned (a network's correction of the linear
+                             extrapolation of the last two solutions), 2 that
+                             extrapolation alone; 1 and 2 fall back to the
+                             previous solution when its first residual is smaller */
     int graph_steps;      /* DEM steps captured per CUDA graph launch; 0 = automatic */
     const char *output_dir; /* directory for .bin/status/conv outputs; NULL = "output" */
     int step_kernel;      /* 0 automatic (the fused persistent step where it applies),

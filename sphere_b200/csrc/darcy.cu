@@ -901,7 +901,7 @@ int Engine::darcy_init()
     if (warm_start) {
         Dd.freec = dalloc<unsigned char>(nx * ny * nz);
         Dd.guess = dalloc<double>(ng);
-        Dd.ws = ws_create(D.nx, D.ny, D.nz, 0x5eed5eedull, warm_start_train);
+        Dd.ws = ws_create(D.nx, D.ny, D.nz, 0x5eed5eedull, warm_start_train, warm_start == 1);
         if (!Dd.ws || !Dd.freec || !Dd.guess)
             return fail(ST_CUDA, "could not set up the learned warm start");
     }

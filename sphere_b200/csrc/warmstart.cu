@@ -425,9 +425,13 @@ __global__ void k_features(int nx, int ny, int nz, const double *p, const double
     dst[1] = *reinterpret_cast<const uint4 *>(&pk[4]);
 }
 
-// guess = p_prev + free * out * dp_scale on interior cells (padded layout)
+// guess = p_prev + free * (last change + out * dp_scale) on interior cells
+// (padded layout): the network corrects the linear extrapolation of the
+// last two solutions; without a network (out null) the guess is that
+// extrapolation
 __global__ void k_compose(int nx, int ny, int nz, const double *p, const float *out,
-                          const unsigned char *freec, const Scalars *sc, double *guess)
+                          const double *dp_base, const unsigned char *freec, const Scalars *sc,
+                          double *guess)
 {
     const unsigned n = (unsigned)nx * ny * nz;
     const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -435,7 +439,10 @@ __global__ void k_compose(int nx, int ny, int nz, const double *p, const float *
     const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((unsigned)nx * ny));
     const unsigned g = didx_ws(nx, ny, x, y, z);
     double v = p[g];
-    if (freec[c] && sc->dp_init) v += (double)out[c] * (double)sc->dp_scale;
+    if (freec[c] && sc->dp_init) {
+        v += dp_base[c];
+        if (out) v += (double)out[c] * (double)sc->dp_scale;
+    }
     guess[g] = v;
 }
 
@@ -443,20 +450,33 @@ __global__ void k_compose(int nx, int ny, int nz, const double *p, const float *
 // (for the running scale) and the change itself (an input of the next
 // prediction)
 __global__ void k_dpmax(int nx, int ny, int nz, const double *p_prev, const double *p_star,
-                        const unsigned char *freec, Scalars *sc, float *dp_last)
+                        const unsigned char *freec, Scalars *sc)
 {
     const unsigned n = (unsigned)nx * ny * nz;
     const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
     float m = 0.0f;
-    if (c < n) {
+    if (c < n && freec[c]) {
         const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((unsigned)nx * ny));
         const unsigned g = didx_ws(nx, ny, x, y, z);
-        const float d = (float)(p_star[g] - p_prev[g]);
-        dp_last[c] = freec[c] ? d : 0.0f;
-        if (freec[c]) m = fabsf(d);
+        m = fabsf((float)(p_star[g] - p_prev[g]));
     }
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) atomicMax(&sc->dpmax_bits, __float_as_uint(m));
+}
+
+// the change of the solve just made, kept for the next extrapolation (FP64)
+// and as the next network input (FP32)
+__global__ void k_dpstore(int nx, int ny, int nz, const double *p_prev, const double *p_star,
+                          const unsigned char *freec, float *dp_last, double *dp_base)
+{
+    const unsigned n = (unsigned)nx * ny * nz;
+    const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((unsigned)nx * ny));
+    const unsigned g = didx_ws(nx, ny, x, y, z);
+    const double dd = freec[c] ? p_star[g] - p_prev[g] : 0.0;
+    dp_base[c] = dd;
+    dp_last[c] = (float)dd;
 }
 
 // running scale of the pressure change: the first solve's maximum, then an
@@ -504,8 +524,8 @@ __global__ void k_weight_sum(const float *partial, unsigned nb, Scalars *sc)
 // squared error of the normalised pressure change, or with
 // target_override the plain mean squared error against that target
 __global__ void k_loss_grad(int nx, int ny, int nz, const double *p_prev, const double *p_star,
-                            const float *out, const unsigned char *freec, Scalars *sc, bf16 *g3,
-                            const float *target_override)
+                            const double *dp_base, const float *out, const unsigned char *freec,
+                            Scalars *sc, bf16 *g3, const float *target_override)
 {
     const unsigned n = (unsigned)nx * ny * nz;
     const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -520,13 +540,17 @@ __global__ void k_loss_grad(int nx, int ny, int nz, const double *p_prev, const 
         } else {
             const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((unsigned)nx * ny));
             const unsigned g = didx_ws(nx, ny, x, y, z);
-            t = (float)((p_star[g] - p_prev[g]) / (double)sc->dp_scale);
+            // the part of the solve's change the extrapolation missed
+            const double base = (dp_base && sc->dp_init) ? dp_base[c] : 0.0;
+            t = (float)((p_star[g] - p_prev[g] - base) / (double)sc->dp_scale);
             w = loss_weight(p_prev[g], fmaxf(__uint_as_float(sc->pmax_bits), 1.0f));
             wsum = fmaxf(sc->wsum, 1e-30f);
         }
         const float e = out[c] - t;
-        grad = 2.0f * w * e / wsum;
-        atomicAdd(&sc->loss, w * e * e / wsum);
+        if (isfinite(e) && isfinite(w)) {   // a degenerate scale trains nothing
+            grad = 2.0f * w * e / wsum;
+            atomicAdd(&sc->loss, w * e * e / wsum);
+        }
     }
     __align__(16) __nv_bfloat162 pk[8];
     pk[0] = __floats2bfloat162_rn(grad, 0.0f);
@@ -566,6 +590,9 @@ struct WarmStart {
     unsigned wgrad_blocks = 0, cells_per_block = 0;
     unsigned char *freec = nullptr;
     float *dp_last = nullptr;       // pressure change of the last solve (free cells)
+    double *dp_base = nullptr;      // the same in FP64: the extrapolation the guess adds
+    bool use_net = true;            // false: the guess is the extrapolation alone
+    int solves = 0;                 // solves recorded by ws_train
     float *wpartial = nullptr;      // per-block loss-weight sums
     Scalars *sc = nullptr;
     int train_iters = 2;            // Adam steps per solve while training
@@ -675,10 +702,11 @@ cudaError_t adam_step(WarmStart &W, cudaStream_t st)
 
 }  // namespace
 
-WarmStart *ws_create(int nx, int ny, int nz, uint64_t seed, int train_solves)
+WarmStart *ws_create(int nx, int ny, int nz, uint64_t seed, int train_solves, bool use_net)
 {
     if (!set_attrs()) return nullptr;
     auto *W = new WarmStart();
+    W->use_net = use_net;
     W->nx = nx; W->ny = ny; W->nz = nz;
     W->ncells = (unsigned)nx * ny * nz;
     W->train_budget = train_solves;
@@ -688,6 +716,7 @@ WarmStart *ws_create(int nx, int ny, int nz, uint64_t seed, int train_solves)
     W->out = W->alloc<float>(W->ncells);
     W->freec = W->alloc<unsigned char>(W->ncells);
     W->dp_last = W->alloc<float>(W->ncells);
+    W->dp_base = W->alloc<double>(W->ncells);
     W->wpartial = W->alloc<float>(blocks(W->ncells, 256));
     W->sc = W->alloc<Scalars>(1);
     W->err = W->alloc<int>(1);
@@ -745,11 +774,14 @@ cudaError_t ws_predict(WarmStart *W, const WSDarcyInputs &in, double *guess, cud
     if ((e = cudaMemsetAsync(W->sc, 0, 16, st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(&W->sc->loss, 0, 4, st)) != cudaSuccess) return e;
     k_stats<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, in.p, in.dphi, W->freec, W->sc);
-    k_features<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, in.p, in.phi, in.dphi,
-                                              W->dp_last, W->sc, W->x0);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = forward(*W, st)) != cudaSuccess) return e;
-    k_compose<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, in.p, W->out, W->freec, W->sc, guess);
+    if (W->use_net) {
+        k_features<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, in.p, in.phi, in.dphi,
+                                                  W->dp_last, W->sc, W->x0);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = forward(*W, st)) != cudaSuccess) return e;
+    }
+    k_compose<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, in.p, W->use_net ? W->out : nullptr,
+                                             W->dp_base, W->freec, W->sc, guess);
     W->last_p_prev = in.p;
     W->predictions += 1;
     return cudaGetLastError();
@@ -759,26 +791,31 @@ cudaError_t ws_train(WarmStart *W, const double *p_prev, const double *p_star, c
 {
     const unsigned n = W->ncells;
     cudaError_t e;
-    // every solve: the running scale and the change the next prediction reads
-    k_dpmax<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, p_star, W->freec, W->sc,
-                                            W->dp_last);
+    // the running scale, including this solve's change
+    k_dpmax<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, p_star, W->freec, W->sc);
     k_dpscale<<<1, 1, 0, st>>>(W->sc);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (W->trained >= W->train_budget) return cudaSuccess;
-    k_weight_partials<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, W->freec, W->sc,
-                                                      W->wpartial);
-    k_weight_sum<<<1, 1, 0, st>>>(W->wpartial, blocks(n, 256), W->sc);
-    for (int it = 0; it < W->train_iters; ++it) {
-        if (it > 0 && (e = forward(*W, st)) != cudaSuccess) return e;
-        if ((e = cudaMemsetAsync(&W->sc->loss, 0, 4, st)) != cudaSuccess) return e;
-        k_loss_grad<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, p_star, W->out,
-                                                    W->freec, W->sc, W->g3, nullptr);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if ((e = backward(*W, st)) != cudaSuccess) return e;
-        if ((e = adam_step(*W, st)) != cudaSuccess) return e;
+    // training (from the second solve on, when an extrapolation exists),
+    // towards what the extrapolation the prediction used missed
+    if (W->use_net && W->solves > 0 && W->trained < W->train_budget) {
+        k_weight_partials<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, W->freec,
+                                                          W->sc, W->wpartial);
+        k_weight_sum<<<1, 1, 0, st>>>(W->wpartial, blocks(n, 256), W->sc);
+        for (int it = 0; it < W->train_iters; ++it) {
+            if (it > 0 && (e = forward(*W, st)) != cudaSuccess) return e;
+            if ((e = cudaMemsetAsync(&W->sc->loss, 0, 4, st)) != cudaSuccess) return e;
+            k_loss_grad<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, p_star, W->dp_base,
+                                                        W->out, W->freec, W->sc, W->g3, nullptr);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            if ((e = backward(*W, st)) != cudaSuccess) return e;
+            if ((e = adam_step(*W, st)) != cudaSuccess) return e;
+        }
+        W->trained += 1;
     }
-    W->trained += 1;
-    return cudaSuccess;
+    // every solve: the change the next prediction extrapolates
+    k_dpstore<<<blocks(n, 256), 256, 0, st>>>(W->nx, W->ny, W->nz, p_prev, p_star, W->freec,
+                                              W->dp_last, W->dp_base);
+    W->solves += 1;
+    return cudaGetLastError();
 }
 
 int ws_error(WarmStart *W, cudaStream_t st)
@@ -848,7 +885,7 @@ int ws_gradients_host(WarmStart *W, const float *x4, const float *target, const 
     s.dp_scale = 1.0f;
     s.dp_init = 1;
     cudaMemcpy(W->sc, &s, sizeof s, cudaMemcpyHostToDevice);
-    k_loss_grad<<<blocks(n, 256), 256>>>(W->nx, W->ny, W->nz, nullptr, nullptr, W->out, W->freec,
+    k_loss_grad<<<blocks(n, 256), 256>>>(W->nx, W->ny, W->nz, nullptr, nullptr, nullptr, W->out, W->freec,
                                          W->sc, W->g3, dt);
     cudaError_t e = backward(*W, nullptr);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -874,7 +911,7 @@ extern "C" {
 int sph_wsnet_create(int nx, int ny, int nz, uint64_t seed, sph_wsnet **out)
 {
     if (!out || nx < 1 || ny < 1 || nz < 1) return -8;
-    sphb::WarmStart *w = sphb::ws_create(nx, ny, nz, seed, 0);
+    sphb::WarmStart *w = sphb::ws_create(nx, ny, nz, seed, 0, true);
     if (!w) return -4;
     *out = new sph_wsnet{w};
     return 0;

@@ -16,16 +16,18 @@ struct WSDarcyInputs {
     const unsigned char *free;
 };
 
-// nullptr when the device cannot run the tensor-core kernels.
-WarmStart *ws_create(int nx, int ny, int nz, uint64_t seed, int train_solves);
+// nullptr when the device cannot run the tensor-core kernels.  use_net =
+// false keeps only the extrapolation (no network, no training).
+WarmStart *ws_create(int nx, int ny, int nz, uint64_t seed, int train_solves, bool use_net);
 void ws_destroy(WarmStart *w);
-// Network prediction for this solve: guess = p + free * predicted change
-// (interior cells of the padded guess array).
+// Prediction for this solve: guess = p + free * (last solve's change +
+// the network's correction), on the interior cells of the padded guess
+// array; the first solve's guess is p.
 cudaError_t ws_predict(WarmStart *w, const WSDarcyInputs &in, double *guess, cudaStream_t st);
-// After a solve: records its pressure change (an input of the next
-// prediction) and the running scale; while the training budget lasts, Adam
-// steps towards the solve's result p_star from p_prev (the inputs of the
-// last prediction).
+// After a solve: while the training budget lasts, Adam steps towards the
+// part of the solve's change (p_star - p_prev) that the extrapolation of
+// the last prediction missed; then records the change (the next
+// extrapolation and network input) and the running scale.
 cudaError_t ws_train(WarmStart *w, const double *p_prev, const double *p_star, cudaStream_t st);
 int ws_trained(const WarmStart *w);
 int ws_predictions(const WarmStart *w);

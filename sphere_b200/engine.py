@@ -170,7 +170,7 @@ def make_opts(fluid=False, precision="faithful", integrator=3, capacity=32, devi
     o.contact_capacity = int(capacity)
     o.device = int(device)
     o.graph_steps = int(graph_steps)
-    o.warm_start = int(bool(warm_start))
+    o.warm_start = int(warm_start) if not isinstance(warm_start, bool) else int(warm_start)
     o.verbose = int(bool(verbose))
     o.output_dir = os.fsencode(output_dir) if output_dir else None
     o.step_kernel = STEP_KERNEL[step_kernel] if isinstance(step_kernel, str) else int(step_kernel)
