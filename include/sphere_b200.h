@@ -54,10 +54,12 @@ typedef struct sph_opts {
     int integrator;       /* 3: three-term Taylor (the reference's TY3), 2: two-term */
     int contact_capacity; /* contact slots per particle; the reference's NC is 32 */
     int warm_start;       /* Darcy start: 0 the previous solution (the reference's),
-                             1 learned (a network's correction of the linear
-                             extrapolation of the last two solutions), 2 that
-                             extrapolation alone; 1 and 2 fall back to the
-                             previous solution when its first residual is smaller */
+                             1 learned (a network's correction of the cubic
+                             extrapolation in time of the last four solutions,
+                             or that extrapolation alone, whichever has the
+                             smaller first residual), 2 that extrapolation
+                             alone; 1 and 2 fall back to the previous solution
+                             when its first residual is smaller */
     int graph_steps;      /* DEM steps captured per CUDA graph launch; 0 = automatic */
     const char *output_dir; /* directory for .bin/status/conv outputs; NULL = "output" */
     int step_kernel;      /* 0 automatic (the fused persistent step where it applies),

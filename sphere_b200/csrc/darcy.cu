@@ -46,7 +46,7 @@ struct DarcyCtl {
     int err;
     // learned warm start: first-iteration residuals of the previous-step
     // guess (0) and of the network's guess (1); solves that used the latter
-    unsigned long long guess_res[2];
+    unsigned long long guess_res[3];
     long long ws_picked;
 };
 
@@ -97,7 +97,8 @@ struct DarcyDev {
     // learned warm start (null when off)
     WarmStart *ws = nullptr;
     unsigned char *freec = nullptr;        // cells the solve may change
-    double *guess = nullptr;               // padded network guess
+    double *guess = nullptr;               // padded guess (extrapolation + network)
+    double *guess_base = nullptr;          // padded extrapolation alone (learned mode)
 };
 
 __device__ __forceinline__ unsigned didx(const DarcyParams &D, int x, int y, int z)
@@ -761,21 +762,29 @@ __global__ void k_guess_residual(DarcyParams D, DarcyFields F, const double *pg,
         atomicMax(&ctl->guess_res[slot], (unsigned long long)__double_as_longlong(a));
 }
 
-// the network's guess replaces the previous-step guess only when its first
-// residual is smaller
-__global__ void k_take_guess(DarcyCtl *ctl, double *p, const double *guess, size_t ng)
+// The solve starts from the candidate with the smallest first residual:
+// the previous solution (slot 0, kept on ties), the guess (slot 1) or the
+// extrapolation alone (slot 2, when guess_base is given).
+__global__ void k_take_guess(DarcyCtl *ctl, double *p, const double *guess, const double *guess_base,
+                             size_t ng)
 {
-    if (!(ctl->guess_res[1] < ctl->guess_res[0])) return;
+    int pick = 0;
+    unsigned long long best = ctl->guess_res[0];
+    if (ctl->guess_res[1] < best) { pick = 1; best = ctl->guess_res[1]; }
+    if (guess_base && ctl->guess_res[2] < best) pick = 2;
+    if (pick == 0) return;
+    const double *src = pick == 1 ? guess : guess_base;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < ng;
          i += (size_t)gridDim.x * blockDim.x)
-        p[i] = guess[i];
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->ws_picked += 1;
+        p[i] = src[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0 && pick == 1) ctl->ws_picked += 1;
 }
 
 __global__ void k_clear_guess_res(DarcyCtl *ctl)
 {
     ctl->guess_res[0] = 0ull;
     ctl->guess_res[1] = 0ull;
+    ctl->guess_res[2] = 0ull;
 }
 
 // findDarcyVelocities, darcy.cuh:1839-1897
@@ -901,6 +910,7 @@ int Engine::darcy_init()
     if (warm_start) {
         Dd.freec = dalloc<unsigned char>(nx * ny * nz);
         Dd.guess = dalloc<double>(ng);
+        if (warm_start == 1) Dd.guess_base = dalloc<double>(ng);
         Dd.ws = ws_create(D.nx, D.ny, D.nz, 0x5eed5eedull, warm_start_train, warm_start == 1);
         if (!Dd.ws || !Dd.freec || !Dd.guess)
             return fail(ST_CUDA, "could not set up the learned warm start");
@@ -971,19 +981,24 @@ cudaError_t Engine::enqueue_fluid()
                                           (unsigned long long)Dd.ng);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (Dd.ws) {
-        // learned initial iterate; the previous-step guess stays unless the
-        // network's has the smaller first residual
+        // predicted initial iterate; the previous solution stays unless a
+        // candidate has the smaller first residual
         k_free_cells<<<cb, 256, 0, stream>>>(D, Dd.ctl, Dd.p_constant, Dd.freec);
         if ((e = cudaMemcpyAsync(Dd.guess, Dd.p, Dd.ng * 8, cudaMemcpyDeviceToDevice, stream)) != cudaSuccess)
             return e;
+        if (Dd.guess_base &&
+            (e = cudaMemcpyAsync(Dd.guess_base, Dd.p, Dd.ng * 8, cudaMemcpyDeviceToDevice, stream)) != cudaSuccess)
+            return e;
         WSDarcyInputs in{Dd.p, Dd.phi, Dd.dphi, Dd.freec};
-        if ((e = ws_predict(Dd.ws, in, Dd.guess, stream)) != cudaSuccess) return e;
+        if ((e = ws_predict(Dd.ws, in, Dd.guess, Dd.guess_base, stream)) != cudaSuccess) return e;
         k_ghost<1><<<cb, 256, 0, stream>>>(D, Dd.guess);
+        if (Dd.guess_base) k_ghost<1><<<cb, 256, 0, stream>>>(D, Dd.guess_base);
         k_clear_guess_res<<<1, 1, 0, stream>>>(Dd.ctl);
         k_guess_residual<<<cb, 256, 0, stream>>>(D, F, Dd.p, Dd.ctl, P.dt, 0);
         k_guess_residual<<<cb, 256, 0, stream>>>(D, F, Dd.guess, Dd.ctl, P.dt, 1);
+        if (Dd.guess_base) k_guess_residual<<<cb, 256, 0, stream>>>(D, F, Dd.guess_base, Dd.ctl, P.dt, 2);
         k_take_guess<<<(unsigned)std::min<size_t>((Dd.ng + 255) / 256, 1024), 256, 0, stream>>>(
-            Dd.ctl, Dd.p, Dd.guess, Dd.ng);
+            Dd.ctl, Dd.p, Dd.guess, Dd.guess_base, Dd.ng);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     // the second buffer starts as a copy (its ghost faces are read too)

@@ -20,14 +20,17 @@ struct WSDarcyInputs {
 // false keeps only the extrapolation (no network, no training).
 WarmStart *ws_create(int nx, int ny, int nz, uint64_t seed, int train_solves, bool use_net);
 void ws_destroy(WarmStart *w);
-// Prediction for this solve: guess = p + free * (last solve's change +
-// the network's correction), on the interior cells of the padded guess
-// array; the first solve's guess is p.
-cudaError_t ws_predict(WarmStart *w, const WSDarcyInputs &in, double *guess, cudaStream_t st);
+// Prediction for this solve: guess = p + free * (the change extrapolated
+// from the last solves + the network's correction), on the interior cells
+// of the padded guess array; the first solve's guess is p.
+// With a network, guess_base (when not null) receives the extrapolation
+// alone, so the solve can start from whichever candidate is best.
+cudaError_t ws_predict(WarmStart *w, const WSDarcyInputs &in, double *guess, double *guess_base,
+                       cudaStream_t st);
 // After a solve: while the training budget lasts, Adam steps towards the
 // part of the solve's change (p_star - p_prev) that the extrapolation of
-// the last prediction missed; then records the change (the next
-// extrapolation and network input) and the running scale.
+// the last prediction missed; then records the change (for the next
+// extrapolation and as a network input) and the running scales.
 cudaError_t ws_train(WarmStart *w, const double *p_prev, const double *p_star, cudaStream_t st);
 int ws_trained(const WarmStart *w);
 int ws_predictions(const WarmStart *w);
