@@ -608,9 +608,13 @@ __device__ __forceinline__ void nl_build_particle(const DevParams &P, const DevS
 #ifndef SPHB_CONTACT_MINB
 #define SPHB_CONTACT_MINB 6
 #endif
+// threads per block of the per-stage contact kernel
+#ifndef SPHB_CONTACT_B
+#define SPHB_CONTACT_B 128
+#endif
 // Contact search and forces of the per-stage path (after k_nl_build).
 template <int PREC, int MODEL>
-__global__ void __launch_bounds__(128, SPHB_CONTACT_MINB) k_contacts(DevParams P, DevState S)
+__global__ void __launch_bounds__(SPHB_CONTACT_B, SPHB_CONTACT_MINB) k_contacts(DevParams P, DevState S)
 {
     extern __shared__ uint32_t srow[];   // blockDim * nc slot partners
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;

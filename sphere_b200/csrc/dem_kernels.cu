@@ -249,7 +249,7 @@ static inline unsigned blocks_for(unsigned n, unsigned b) { return (n + b - 1) /
 cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cudaStream_t st)
 {
     if (P.np == 0) return cudaSuccess;
-    const unsigned B = 128;
+    const unsigned B = SPHB_CONTACT_B;
     dim3 grid(blocks_for(P.np, B));
     if (P.contactmodel == 2) {
         size_t smem = (size_t)B * P.nc * sizeof(uint32_t);

@@ -10,7 +10,7 @@ namespace sphb {
 cudaError_t launch_contacts_mixed(const DevParams &P, const DevState &S, cudaStream_t st)
 {
     if (P.np == 0) return cudaSuccess;
-    const unsigned B = 128;
+    const unsigned B = SPHB_CONTACT_B;
     dim3 grid((P.np + B - 1) / B);
     if (P.contactmodel == 2) {
         size_t smem = (size_t)B * P.nc * sizeof(uint32_t);
