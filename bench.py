@@ -148,6 +148,21 @@ def measure(d, precision, args, flush):
                  "ms_per_step": 1e3 * step_s / args.steps}
 
 
+def shear_report(d, eng, info):
+    """The shear test's observables after the steps run so far: the
+    effective shear stress (python/sphere.py:6406-6432: minus the x forces
+    on the fixed particles moving in +x, over the top area) and the dilation
+    in mean particle diameters (:6786-6810)."""
+    vel = eng.get("vel")
+    force = eng.get("force")
+    moving = (vel[:, 3] > 0.0) & (vel[:, 0] > 0.0)
+    tau = float(-force[moving, 0].sum() / (d.L[0] * d.L[1]))
+    w_x = float(eng.get("walls_nx")[0, 3])
+    d_bar = float(numpy.mean(d.radius) * 2.0)
+    return {"dem_steps": int(info.iter), "shear_stress_pa": tau,
+            "dilation_mean_diameters": (w_x - float(d.w_x[0])) / d_bar}
+
+
 def force_error(d):
     """Normwise relative force error of the mixed mode against FP64 after
     one step from the same state: ||F_mixed - F_fp64|| / ||F_fp64||."""
@@ -213,6 +228,7 @@ def run_gpu(args):
         e2e_times.append(t1 - t0)
     e2e_value = n * INTERVAL * len(e2e_times) / float(numpy.sum(e2e_times))
     info = eng.info()
+    shear = shear_report(d, eng, info)
     eng.close()
 
     peak, peak_kind = load_peaks()
@@ -268,6 +284,7 @@ def run_gpu(args):
                                   "bonds": prof.bonds_ms, "integrate": prof.integrate_ms,
                                   "step": prof.step_ms},
         "resorts": int(info.resorts),
+        "shear_observables": shear,
         "step_path": {"kernel": "persistent" if info.step_path == 1 else "per-stage",
                       "threads": int(info.step_threads), "grid": int(info.step_grid),
                       "autotuned": bool(info.tuned)},
@@ -286,6 +303,8 @@ def run_gpu(args):
         out["batch"] = batch_leg(args)
     if args.large_particles > 0:
         out["large"] = large_leg(args)
+    if args.settle_steps > 0:
+        out["settle"] = settle_leg(args)
     return out
 
 
@@ -367,6 +386,31 @@ def batch_leg(args):
         "ms_per_step": 1e3 * step_s / len(times), "dem_steps_per_step": interval,
         "launch": cfg, "autotuner_trials": len(trials),
         "best_trial_ms_per_step": min(t["ms_per_step"] for t in trials) if trials else None,
+    }
+
+
+def settle_leg(args):
+    """Plain FP64 dry settling (the configuration the reference itself runs):
+    10,000 spheres on the first sites of a 22 x 22 x 21 lattice, spacing
+    0.025 m, jitter +/-0.002 m, radii U(0.009, 0.011) m, periodic x/y, linear
+    contact k_n = k_t = 1.16e7 N/m, mu = 0.5, run for its 20,000 steps from
+    the lattice; faithful FP64."""
+    from sphere_b200 import configs
+    from sphere_b200.engine import Engine
+    d = configs.settling_lattice(n=10000, seed=SEED)
+    steps = args.settle_steps
+    with Engine(d, precision="faithful", graph_steps=100) as eng:
+        ms = eng.step_timed(steps)
+        info = eng.info()
+        zbar = mean_contacts(eng, d.np)
+    return {
+        "workload": "dry settling, N=10000 on a 22x22x21 lattice (spacing 0.025 m, jitter 0.002 m), "
+                    "radii U(0.009, 0.011) m, k_n = k_t = 1.16e7 N/m, mu = 0.5, periodic x/y, "
+                    "faithful FP64, from the lattice",
+        "dem_steps": steps, "particle_steps_per_s": d.np * steps / (ms * 1e-3),
+        "us_per_dem_step": 1e3 * ms / steps, "resorts": int(info.resorts),
+        "mean_contacts_per_particle_at_end": zbar,
+        "step_path": "persistent" if info.step_path == 1 else "per-stage",
     }
 
 
@@ -504,8 +548,10 @@ def main():
                     help="spheres of the large cohesive-packing leg (0 skips it)")
     ap.add_argument("--large-steps", type=int, default=5,
                     help="timed calls of 20 DEM steps in the large leg")
-    ap.add_argument("--legs", default="shear,darcy,batch,large",
-                    help="comma list of legs to run: shear (the headline), darcy, batch, large")
+    ap.add_argument("--settle-steps", type=int, default=20000,
+                    help="DEM steps of the 10,000-sphere settling leg (0 skips it)")
+    ap.add_argument("--legs", default="shear,darcy,batch,large,settle",
+                    help="comma list of legs to run: shear (the headline), darcy, batch, large, settle")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -528,6 +574,8 @@ def main():
             out["batch"] = batch_leg(args)
         if "large" in legs and args.large_particles > 0:
             out["large"] = large_leg(args)
+        if "settle" in legs and args.settle_steps > 0:
+            out["settle"] = settle_leg(args)
         print(json.dumps(out), flush=True)
         return 0
     if "darcy" not in legs:
@@ -536,6 +584,8 @@ def main():
         args.batch_boxes = 0
     if "large" not in legs:
         args.large_particles = 0
+    if "settle" not in legs:
+        args.settle_steps = 0
     print(json.dumps(run_gpu(args)), flush=True)
     return 0
 
