@@ -305,6 +305,8 @@ def run_gpu(args):
         out["large"] = large_leg(args)
     if args.settle_steps > 0:
         out["settle"] = settle_leg(args)
+    if args.render:
+        out["render"] = render_leg(args, d)
     return out
 
 
@@ -387,6 +389,25 @@ def batch_leg(args):
         "launch": cfg, "autotuner_trials": len(trials),
         "best_trial_ms_per_step": min(t["ms_per_step"] for t in trials) if trials else None,
     }
+
+
+def render_leg(args, d):
+    """The ray tracer (``sphere --render``) on the headline packing at the
+    reference's defaults: 800 x 800 pixels, pressure colour map."""
+    from sphere_b200.engine import Engine
+    import time as _t
+    with Engine(d, precision="mixed") as eng:
+        eng.step(10)
+        eng.render(method=1, width=800, height=800)      # warm-up
+        t0 = _t.perf_counter()
+        reps = 3
+        for _ in range(reps):
+            eng.render(method=1, width=800, height=800)
+        s = (_t.perf_counter() - t0) / reps
+    tests = 800 * 800 * d.np
+    return {"workload": f"ray-traced image, 800x800 pixels, N={d.np} spheres, pressure colour map",
+            "ms_per_image": 1e3 * s, "ray_sphere_tests_per_s": tests / s,
+            "note": "wall time of the whole call (state read-back, camera, kernels, image copy)"}
 
 
 def settle_leg(args):
@@ -548,10 +569,13 @@ def main():
                     help="spheres of the large cohesive-packing leg (0 skips it)")
     ap.add_argument("--large-steps", type=int, default=5,
                     help="timed calls of 20 DEM steps in the large leg")
+    ap.add_argument("--render", type=int, default=1,
+                    help="1: time the ray tracer on the headline packing (0 skips it)")
     ap.add_argument("--settle-steps", type=int, default=20000,
                     help="DEM steps of the 10,000-sphere settling leg (0 skips it)")
-    ap.add_argument("--legs", default="shear,darcy,batch,large,settle",
-                    help="comma list of legs to run: shear (the headline), darcy, batch, large, settle")
+    ap.add_argument("--legs", default="shear,darcy,batch,large,settle,render",
+                    help="comma list of legs to run: shear (the headline), darcy, batch, large, "
+                         "settle, render")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -576,6 +600,8 @@ def main():
             out["large"] = large_leg(args)
         if "settle" in legs and args.settle_steps > 0:
             out["settle"] = settle_leg(args)
+        if "render" in legs and args.render:
+            out["render"] = render_leg(args, workload(args.particles))
         print(json.dumps(out), flush=True)
         return 0
     if "darcy" not in legs:
@@ -586,6 +612,8 @@ def main():
         args.large_particles = 0
     if "settle" not in legs:
         args.settle_steps = 0
+    if "render" not in legs:
+        args.render = 0
     print(json.dumps(run_gpu(args)), flush=True)
     return 0
 

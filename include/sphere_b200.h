@@ -223,6 +223,19 @@ int sph_porosity(sph_engine *e, int z_slices, double *z_pos, double *porosity);
 int sph_overlaps(sph_engine *e, uint32_t *pairs, double *delta, uint64_t capacity,
                  uint64_t *count);
 
+/* Ray-traced image of the current state into rgba (width x height x 4
+ * bytes, pixel i + j * width, alpha 255), replacing DEM::render
+ * (src/raytracer.cuh: rayInitPerspective, rayIntersectSpheres and
+ * rayIntersectSpheresColormap with the camera of DEM::cameraInit) behind
+ * `sphere --render`; the caller writes the PPM (DEM::writePPM,
+ * src/file_io.cpp:734-757).  method 0: shaded spheres; 1 pressure,
+ * 2 speed, 3 angular speed, 4 x displacement, 5 rotation, coloured over
+ * [0, max_val] (fixed particles grey); with lower_cutoff > 0 only free
+ * particles whose value exceeds it are drawn.  The reference's defaults
+ * are method 1, max_val 1e3, 800 x 800. */
+int sph_render(sph_engine *e, int method, float max_val, float lower_cutoff, uint32_t width,
+               uint32_t height, unsigned char *rgba);
+
 /* Message for the last non-zero status of this handle (never NULL). */
 const char *sph_last_error(sph_engine *e);
 

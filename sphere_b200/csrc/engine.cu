@@ -1046,6 +1046,12 @@ int sph_porosity(sph_engine *e, int z_slices, double *z_pos, double *porosity)
     return e ? e->e->porosity_profile(z_slices, z_pos, porosity) : SPH_ERR_ARG;
 }
 
+int sph_render(sph_engine *e, int method, float max_val, float lower_cutoff, uint32_t width,
+               uint32_t height, unsigned char *rgba)
+{
+    return e ? e->e->render(method, max_val, lower_cutoff, width, height, rgba) : SPH_ERR_ARG;
+}
+
 int sph_overlaps(sph_engine *e, uint32_t *pairs, double *delta, uint64_t capacity, uint64_t *count)
 {
     return e ? e->e->overlaps(pairs, delta, capacity, count) : SPH_ERR_ARG;

@@ -117,6 +117,8 @@ public:
     int energy(const char *method, double *out);
     int porosity_profile(int z_slices, double *z_pos, double *porosity);
     int overlaps(uint32_t *pairs, double *delta, uint64_t cap, uint64_t *count);
+    int render(int method, float max_val, float lower_cutoff, unsigned width, unsigned height,
+               unsigned char *rgba);
 
     // mixed precision
     int mixed_init();

@@ -118,6 +118,8 @@ def lib() -> ctypes.CDLL:
     L.sph_check_file.restype = ctypes.c_int
     L.sph_energy.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
     L.sph_time_sort.argtypes = [P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.sph_render.argtypes = [P, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_uint32,
+                             ctypes.c_uint32, ctypes.c_void_p]
     L.sph_porosity.argtypes = [P, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
     L.sph_overlaps.argtypes = [P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                ctypes.POINTER(ctypes.c_uint64)]
@@ -302,6 +304,15 @@ class Engine:
         self._check(lib().sph_porosity(self._h, int(slices), z.ctypes.data, phi.ctypes.data))
         return phi, z
 
+    def render(self, method=1, max_val=1.0e3, lower_cutoff=0.0, width=800, height=800):
+        """Ray-traced image of the current state (``sphere --render``,
+        src/raytracer.cuh): a (height, width, 4) uint8 RGBA array, row j
+        holding pixels i + j * width."""
+        img = numpy.empty((int(height), int(width), 4), dtype=numpy.uint8)
+        self._check(lib().sph_render(self._h, int(method), float(max_val), float(lower_cutoff),
+                                     int(width), int(height), img.ctypes.data))
+        return img
+
     def find_overlaps(self):
         """sim.findOverlaps() (python/sphere.py:4868-4883): returns (pairs,
         overlaps), pairs a 2 x M int32 array of particle indices (i < j) and
@@ -324,6 +335,16 @@ class Engine:
         pairs, _ = self.find_overlaps()
         return (numpy.bincount(pairs[0], minlength=self.np)
                 + numpy.bincount(pairs[1], minlength=self.np))
+
+
+def write_ppm(path, img):
+    """Writes an RGBA image as a binary PPM (P6, the RGB channels), pixels in
+    the order DEM::writePPM writes them (src/file_io.cpp:734-757)."""
+    img = numpy.ascontiguousarray(img)
+    h, w = img.shape[:2]
+    with open(path, "wb") as f:
+        f.write(f"P6 {w} {h} 255\n".encode())
+        f.write(img[:, :, :3].tobytes())
 
 
 def check_file(path, fluid=False):
