@@ -359,21 +359,30 @@ int Engine::ensure_graph()
     }
     if (graph_exec || graph_steps <= 1 || graph_failed) return ST_OK;
     graph_view = cur_view;
+    graph_exec = capture_steps(graph_steps);
+    if (!graph_exec) graph_failed = true;
+    return ST_OK;
+}
+
+// A CUDA graph of k per-stage DEM steps on the current state view, or null
+// when capture or instantiation fails (the caller then steps eagerly).
+cudaGraphExec_t Engine::capture_steps(int k)
+{
     cudaGraph_t g = nullptr;
+    cudaGraphExec_t x = nullptr;
     cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) { graph_failed = true; cudaGetLastError(); return ST_OK; }
-    for (int i = 0; i < graph_steps && e == cudaSuccess; ++i) e = enqueue_step();
+    if (e != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    for (int i = 0; i < k && e == cudaSuccess; ++i) e = enqueue_step();
     cudaError_t e2 = cudaStreamEndCapture(stream, &g);
     if (e != cudaSuccess || e2 != cudaSuccess || !g) {
         if (g) cudaGraphDestroy(g);
-        graph_failed = true;
         cudaGetLastError();
-        return ST_OK;
+        return nullptr;
     }
-    e = cudaGraphInstantiate(&graph_exec, g, 0);
+    e = cudaGraphInstantiate(&x, g, 0);
     cudaGraphDestroy(g);
-    if (e != cudaSuccess) { graph_exec = nullptr; graph_failed = true; cudaGetLastError(); }
-    return ST_OK;
+    if (e != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    return x;
 }
 
 int Engine::step(uint64_t n)

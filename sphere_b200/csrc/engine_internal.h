@@ -86,6 +86,9 @@ public:
     cudaError_t enqueue_fluid();
     int profile(uint64_t n, struct sph_profile *out);
     int ensure_graph();
+    cudaGraphExec_t capture_steps(int k);
+    cudaError_t launch_trial_steps(cudaGraphExec_t g, uint64_t n);
+    int stages_after(uint64_t n);
     int step(uint64_t n);
     int step_stages(uint64_t n);
     void advance_host_clock(uint64_t n);

@@ -159,27 +159,34 @@ int Engine::step_persistent(uint64_t n)
         float best = 1e30f;
         int best_cand = D.shape;
         int rc = ST_OK;
+        cudaGraphExec_t trial_graph = nullptr;
         for (int cand = 0; cand < ncand && rc == ST_OK; ++cand) {
             const bool stages = cand == kNumPersistShapes;
             unsigned g = stages ? 1 : persist_grid(cand);
             if (!g) continue;
             if (stages) {
-                // warm the per-stage path (eager first step, graph capture)
-                rc = step_stages(trial);
-                done += trial;
+                // warm the per-stage path: the eager first step, then the
+                // trial steps as one graph (as they run in production; eager
+                // launches would time the host, not the kernels)
+                rc = step_stages(1);
+                done += 1;
                 if (rc) break;
+                trial_graph = capture_steps((int)trial);
+                cudaError_t e = launch_trial_steps(trial_graph, trial);
+                if (e != cudaSuccess) rc = cuda_fail(e, "step");
+                done += trial;
+                if (rc || (rc = stages_after(trial))) break;
             }
             cudaEventRecord(a, stream);
-            cudaError_t e = stages ? cudaSuccess : persist_launch(trial, cand, g);
-            if (stages) rc = step_stages(trial);
+            cudaError_t e = stages ? launch_trial_steps(trial_graph, trial) : persist_launch(trial, cand, g);
             cudaEventRecord(b, stream);
-            if (e != cudaSuccess) rc = cuda_fail(e, "persistent step");
+            if (e != cudaSuccess) rc = cuda_fail(e, stages ? "step" : "persistent step");
             if (rc) break;
             cudaEventSynchronize(b);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, a, b);
             done += trial;
-            if (!stages && (rc = persist_after(trial))) break;
+            if ((rc = stages ? stages_after(trial) : persist_after(trial))) break;
             if (ms < best) {
                 best = ms;
                 best_cand = cand;
@@ -187,6 +194,7 @@ int Engine::step_persistent(uint64_t n)
         }
         cudaEventDestroy(a);
         cudaEventDestroy(b);
+        if (trial_graph) cudaGraphExecDestroy(trial_graph);
         if (rc) return rc;
         D.tuned = true;
         if (best_cand == kNumPersistShapes) {
@@ -202,6 +210,24 @@ int Engine::step_persistent(uint64_t n)
         return persist_after(n - done);
     }
     return ST_OK;
+}
+
+// Enqueues the n per-stage steps of a tuning trial: one replay of the
+// n-step graph, or eager launches when it could not be captured.  Nothing
+// waits on the host, so the events around it time the device alone.
+cudaError_t Engine::launch_trial_steps(cudaGraphExec_t g, uint64_t n)
+{
+    if (g) return cudaGraphLaunch(g, stream);
+    cudaError_t e = cudaSuccess;
+    for (uint64_t i = 0; i < n && e == cudaSuccess; ++i) e = enqueue_step();
+    return e;
+}
+
+// After n per-stage trial steps: the host clock and device errors.
+int Engine::stages_after(uint64_t n)
+{
+    advance_host_clock(n);
+    return poll_errors("step");
 }
 
 // After a launch of n steps: advance the host mirrors, pick up the current
