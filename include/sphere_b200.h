@@ -114,6 +114,16 @@ typedef enum sph_field {
     SPH_F_BONDS_DELTA,  /* nb0 x 4 doubles (t.x, t.y, t.z, n) */
     SPH_F_BONDS_OMEGA,
     SPH_F_VELOCITY_STATE, /* 1 int64: rate-state velocity step state (device.cu:2461-2469) */
+    /* Navier-Stokes runs (cfd_solver 0) also answer the SPH_F_DARCY_P, _PHI,
+     * _DPHI, _V (cell-centre velocity), _F_P (pressure force), _ITERS and
+     * _ITERS_TOTAL fields above (navierstokes.cuh device arrays) */
+    SPH_F_NS_EPSILON,   /* nx*ny*nz doubles: pressure change of the last projection */
+    SPH_F_NS_NORM,      /* nx*ny*nz doubles: normalised Jacobi residuals */
+    SPH_F_NS_V_FACE,    /* (nx+1)(ny+1)(nz+1) x 3 doubles: staggered face velocities
+                           v_x, v_y, v_z at faces 0..n per axis, x fastest */
+    SPH_F_NS_F_D,       /* np x 4 doubles: drag force on each particle */
+    SPH_F_NS_F_V,       /* np x 4 doubles: viscous force */
+    SPH_F_NS_F_SUM,     /* np x 4 doubles: total fluid force */
     SPH_F_COUNT
 } sph_field;
 

@@ -69,6 +69,12 @@ def lib():
 
 
 def _shape(name, nbytes):
+    if name in ("ns_f_d", "ns_f_p", "ns_f_v", "ns_f_sum"):
+        return numpy.float64, (nbytes // 32, 4)
+    if name in ("ns_nijac_last", "ns_nijac_total", "ns_converged"):
+        return numpy.int64, (nbytes // 8,)
+    if name in ("ns_v", "ns_F_pf", "ns_v_face"):
+        return numpy.float64, (nbytes // 24, 3)
     if name in _FIELD4:
         return numpy.float64, (nbytes // 32, 4)
     if name in _SLOT4:

@@ -169,6 +169,7 @@ void DEM::transferToGlobalDeviceMemory(int)
     std::memcpy(dev_walls_mvfd, walls.mvfd, sizeof(Float4) * walls.nw);
     if (walls.nw) std::memcpy(dev_walls_tau_x, walls.tau_x, sizeof(Float));
     if (fluid == 1 && cfd_solver == 1) transferDarcyToGlobalDeviceMemory(0);
+    if (fluid == 1 && cfd_solver == 0) transferNStoGlobalDeviceMemory(0);
 }
 
 void DEM::transferFromGlobalDeviceMemory()
@@ -194,6 +195,7 @@ void DEM::transferFromGlobalDeviceMemory()
     std::memcpy(walls.nx, dev_walls_nx, sizeof(Float4) * walls.nw);
     std::memcpy(walls.mvfd, dev_walls_mvfd, sizeof(Float4) * walls.nw);
     if (fluid == 1 && cfd_solver == 1) transferDarcyFromGlobalDeviceMemory(0);
+    if (fluid == 1 && cfd_solver == 0) transferNSfromGlobalDeviceMemory(0);
 }
 
 void DEM::freeGlobalDeviceMemory() {}
@@ -207,6 +209,7 @@ struct RefRun {
     long nijac_last;
     long nijac_total;
     double filetimeclock;
+    int ns_converged;
 };
 
 /* summation (integration.cuh:309-341) uses a 256-wide shared-memory tree
@@ -323,6 +326,143 @@ static void ref_darcy(RefRun *r)
     }
 }
 
+/* The Navier-Stokes block of DEM::startTime, device.cu:1213-1898
+ * (cfd_solver 0, CFD_DEM_COUPLING), kernels launched one thread at a time. */
+static void ref_ns(RefRun *r)
+{
+    DEM &d = *r->dem;
+    NavierStokes &ns = d.ns;
+    unsigned np = d.np;
+    unsigned tpb = 256, bpg = idiv_up(np, tpb);
+    dim3 blk(8, 8, 8);
+    dim3 grd(idiv_up(d.grid.num[0], 8), idiv_up(d.grid.num[1], 8), idiv_up(d.grid.num[2], 8));
+    dim3 grdf(idiv_up(d.grid.num[0] + 1, 8), idiv_up(d.grid.num[1] + 1, 8), idiv_up(d.grid.num[2] + 1, 8));
+    const int bb = ns.bc_bot, bt = ns.bc_top;
+    const unsigned iter = (unsigned)r->iter;
+    const Float dp_dz = fabs(ns.rho_f * d.params.g[2] * d.grid.L[2] / d.grid.num[2]);
+    auto ghost = [&](Float *f) { launch3(grd, blk, [&] { setNSghostNodes<Float>(f, bb, bt); }); };
+    auto ghost3 = [&](Float3 *f) { launch3(grd, blk, [&] { setNSghostNodes<Float3>(f, bb, bt); }); };
+    auto ghostf = [&](Float *x, Float *y, Float *z) {
+        launch3(grdf, blk, [&] { setNSghostNodesFace<Float>(x, y, z, bb, bt); });
+    };
+    launch3(grd, blk, [&] {
+        findPorositiesVelocitiesDiametersSpherical(d.dev_cellStart, d.dev_cellEnd, d.dev_x_sorted,
+                                                   d.dev_vel_sorted, d.dev_ns_phi, d.dev_ns_dphi,
+                                                   d.dev_ns_vp_avg, d.dev_ns_d_avg, iter, np, ns.c_phi);
+    });
+    if (iter == 0) {
+        ghost3(d.dev_ns_v);
+        launch3(grdf, blk, [&] { interpolateCenterToFace(d.dev_ns_v, d.dev_ns_v_x, d.dev_ns_v_y, d.dev_ns_v_z); });
+    }
+    ghostf(d.dev_ns_v_x, d.dev_ns_v_y, d.dev_ns_v_z);
+    launch3(grdf, blk, [&] {
+        findFaceDivTau(d.dev_ns_v_x, d.dev_ns_v_y, d.dev_ns_v_z, ns.mu, d.dev_ns_div_tau_x,
+                       d.dev_ns_div_tau_y, d.dev_ns_div_tau_z);
+    });
+    ghostf(d.dev_ns_div_tau_x, d.dev_ns_div_tau_y, d.dev_ns_div_tau_z);
+    ghost(d.dev_ns_p);
+    ghost(d.dev_ns_phi);
+    if (np > 0) {
+        launch(bpg, tpb, [&] {
+            findInteractionForce(d.dev_x, d.dev_vel, d.dev_ns_phi, d.dev_ns_p, d.dev_ns_v_x, d.dev_ns_v_y,
+                                 d.dev_ns_v_z, d.dev_ns_div_tau_x, d.dev_ns_div_tau_y, d.dev_ns_div_tau_z,
+                                 ns.mu, ns.rho_f, d.dev_ns_f_pf, d.dev_force, d.dev_ns_f_d, d.dev_ns_f_p,
+                                 d.dev_ns_f_v, d.dev_ns_f_sum);
+        });
+        ghost(d.dev_ns_p);
+        launch3(grd, blk, [&] {
+            applyInteractionForceToFluid(d.dev_gridParticleIndex, d.dev_cellStart, d.dev_cellEnd,
+                                         d.dev_ns_f_pf, d.dev_ns_F_pf);
+        });
+        ghost3(d.dev_ns_F_pf);
+    }
+    if ((r->iter % ns.ndem) != 0) return;
+    Float pressure = ns.p[d.idx(0, 0, ns.nz - 1)];
+    Float epsilon_value = pressure - ns.beta * pressure;
+    launch3(grd, blk, [&] { setNSepsilonTop(d.dev_ns_epsilon, d.dev_ns_epsilon_new, epsilon_value); });
+    if (d.walls.nw > 0 && (d.walls.wmode[0] == 1 || d.walls.wmode[0] == 3)) {
+        r->wall0_iz = d.walls.nx->w / (d.grid.L[2] / d.grid.num[2]);
+        launch3(grd, blk, [&] {
+            setNSepsilonAtTopWall(d.dev_ns_epsilon, d.dev_ns_epsilon_new, r->wall0_iz, epsilon_value, dp_dz);
+        });
+    }
+    const unsigned wall0_iz = r->wall0_iz;
+    if ((ns.p_mod_A > 1.0e-5 || ns.p_mod_A < -1.0e-5) && ns.p_mod_f > 1.0e-7) {
+        Float new_pressure = ns.p[d.idx(0, 0, ns.nz - 1)] +
+                             ns.p_mod_A * sin(2.0 * M_PI * ns.p_mod_f * d.time.current + ns.p_mod_phi);
+        launch3(grd, blk, [&] {
+            setUpperPressureNS(d.dev_ns_p, d.dev_ns_epsilon, d.dev_ns_epsilon_new, ns.beta, new_pressure);
+        });
+    }
+    ghost(d.dev_ns_p);
+    ghostf(d.dev_ns_v_p_x, d.dev_ns_v_p_y, d.dev_ns_v_p_z);
+    ghost(d.dev_ns_phi);
+    ghost(d.dev_ns_dphi);
+    launch3(grd, blk, [&] { interpolateFaceToCenter(d.dev_ns_v_x, d.dev_ns_v_y, d.dev_ns_v_z, d.dev_ns_v); });
+    ghost3(d.dev_ns_v);
+    launch3(grd, blk, [&] { findNSdivphiviv(d.dev_ns_phi, d.dev_ns_v, d.dev_ns_div_phi_vi_v); });
+    ghost3(d.dev_ns_div_phi_vi_v);
+    launch3(grdf, blk, [&] {
+        findPredNSvelocities(d.dev_ns_p, d.dev_ns_v_x, d.dev_ns_v_y, d.dev_ns_v_z, d.dev_ns_phi, d.dev_ns_dphi,
+                             d.dev_ns_div_tau_x, d.dev_ns_div_tau_y, d.dev_ns_div_tau_z,
+                             d.dev_ns_div_phi_vi_v, bb, bt, ns.beta, d.dev_ns_F_pf, ns.ndem, wall0_iz,
+                             ns.c_v, ns.mu, ns.rho_f, d.dev_ns_v_p_x, d.dev_ns_v_p_y, d.dev_ns_v_p_z);
+    });
+    ghostf(d.dev_ns_v_p_x, d.dev_ns_v_p_y, d.dev_ns_v_p_z);
+    launch3(grd, blk, [&] { interpolateFaceToCenter(d.dev_ns_v_p_x, d.dev_ns_v_p_y, d.dev_ns_v_p_z, d.dev_ns_v_p); });
+    if (iter == 0) {
+        pressure = ns.p[d.idx(2, 2, 2)];
+        epsilon_value = pressure - ns.beta * pressure;
+        launch3(grd, blk, [&] { setNSepsilonInterior(d.dev_ns_epsilon, epsilon_value); });
+        launch3(grd, blk, [&] { setNSnormZero(d.dev_ns_norm); });
+        pressure = ns.p[d.idx(0, 0, 0)];
+        epsilon_value = pressure - ns.beta * pressure;
+        launch3(grd, blk, [&] { setNSepsilonBottom(d.dev_ns_epsilon, d.dev_ns_epsilon_new, epsilon_value); });
+        ghost(d.dev_ns_epsilon);
+    }
+    double max_norm_res = 0.0;
+    long done = -1;
+    int conv = 0;
+    for (unsigned int nijac = 0; nijac < ns.maxiter; ++nijac) {
+        launch3(grd, blk, [&] {
+            findNSforcing(d.dev_ns_epsilon, d.dev_ns_phi, d.dev_ns_dphi, d.dev_ns_v_p, d.dev_ns_v_p_x,
+                          d.dev_ns_v_p_y, d.dev_ns_v_p_z, nijac, ns.ndem, ns.c_v, ns.rho_f, d.dev_ns_f1,
+                          d.dev_ns_f2, d.dev_ns_f);
+        });
+        ghost(d.dev_ns_epsilon);
+        launch3(grd, blk, [&] {
+            jacobiIterationNS(d.dev_ns_epsilon, d.dev_ns_epsilon_new, d.dev_ns_norm, d.dev_ns_f, bb, bt,
+                              ns.theta, wall0_iz, dp_dz);
+        });
+        launch3(grd, blk, [&] { copyValues<Float>(d.dev_ns_epsilon_new, d.dev_ns_epsilon); });
+        done = nijac;
+        if (nijac % nijacnorm == 0) {
+            d.transferNSnormFromGlobalDeviceMemory();
+            max_norm_res = d.maxNormResNS();
+        }
+        if (max_norm_res < ns.tolerance) {
+            conv = 1;
+            ghost(d.dev_ns_epsilon);
+            if (ns.gamma > 0.0) {
+                launch3(grd, blk, [&] { smoothing<Float>(d.dev_ns_epsilon, ns.gamma, bb, bt); });
+                ghost(d.dev_ns_epsilon);
+            }
+            break;
+        }
+    }
+    r->nijac_last = done;
+    r->nijac_total += done + 1;
+    r->ns_converged = conv;
+    launch3(grd, blk, [&] { updateNSpressure(d.dev_ns_epsilon, ns.beta, d.dev_ns_p); });
+    launch3(grdf, blk, [&] {
+        updateNSvelocity(d.dev_ns_v_p_x, d.dev_ns_v_p_y, d.dev_ns_v_p_z, d.dev_ns_phi, d.dev_ns_epsilon,
+                         ns.beta, bb, bt, ns.ndem, ns.c_v, ns.rho_f, wall0_iz, iter, d.dev_ns_v_x,
+                         d.dev_ns_v_y, d.dev_ns_v_z);
+    });
+    ghostf(d.dev_ns_v_p_x, d.dev_ns_v_p_y, d.dev_ns_v_p_z);
+    launch3(grd, blk, [&] { interpolateFaceToCenter(d.dev_ns_v_x, d.dev_ns_v_y, d.dev_ns_v_z, d.dev_ns_v); });
+}
+
 static int ref_one_step(RefRun *r)
 {
     DEM &d = *r->dem;
@@ -372,6 +512,7 @@ static int ref_one_step(RefRun *r)
         }
     }
     if (d.fluid == 1 && d.cfd_solver == 1) ref_darcy(r);
+    if (d.fluid == 1 && d.cfd_solver == 0) ref_ns(r);
     if (np > 0) {
         if (d.walls.nw > 0 && d.walls.wmode[0] == 3) {
             launch(bpg, tpb, [&] {
@@ -420,7 +561,23 @@ void *ref_open(const char *path, int fluid)
     /* DEM(inputbin, verbosity, checkVals, dry, initCuda, transferConstMem,
      *     fluidFlow, device) -- sphere.h */
     DEM *d = new DEM(std::string(path), 0, 1, 0, 1, 1, fluid, 0);
-    RefRun *r = new RefRun{d, 0, 1, 10000000u, 0, 0, 0.0};
+    RefRun *r = new RefRun{d, 0, 1, 10000000u, 0, 0, 0.0, 0};
+    if (fluid && d->cfd_solver == 0) {
+        // deterministic ghost nodes (the reference copies them from
+        // uninitialised host memory)
+        unsigned nx = d->grid.num[0], ny = d->grid.num[1], nz = d->grid.num[2];
+        for (int z = -1; z <= (int)nz; ++z)
+            for (int y = -1; y <= (int)ny; ++y)
+                for (int x = -1; x <= (int)nx; ++x) {
+                    bool ghost = x < 0 || y < 0 || z < 0 || x == (int)nx || y == (int)ny || z == (int)nz;
+                    if (!ghost) continue;
+                    unsigned i = d->idx(x, y, z);
+                    d->dev_ns_p[i] = 0.0;
+                    d->dev_ns_phi[i] = 0.0;
+                    d->dev_ns_dphi[i] = 0.0;
+                    d->dev_ns_v[i] = make_double3(0.0, 0.0, 0.0);
+                }
+    }
     if (fluid && d->cfd_solver == 1) {
         // deterministic ghost cells (the reference leaves them uninitialised)
         unsigned nx = d->grid.num[0], ny = d->grid.num[1], nz = d->grid.num[2];
@@ -457,6 +614,13 @@ int ref_step(void *h, long n)
 int ref_write(void *h, const char *path)
 {
     RefRun *r = (RefRun *)h;
+    DEM &d = *r->dem;
+    if (d.fluid == 1 && d.cfd_solver == 0) {
+        /* device.cu:2586-2593 */
+        dim3 blk(8, 8, 8);
+        dim3 grd(idiv_up(d.grid.num[0], 8), idiv_up(d.grid.num[1], 8), idiv_up(d.grid.num[2], 8));
+        launch3(grd, blk, [&] { interpolateFaceToCenter(d.dev_ns_v_x, d.dev_ns_v_y, d.dev_ns_v_z, d.dev_ns_v); });
+    }
     r->dem->transferFromGlobalDeviceMemory();
     r->dem->writebin(path);
     return 0;
@@ -524,6 +688,52 @@ long ref_get(void *h, const char *name, void *dst, size_t bytes)
                         for (int c = 0; c < comps; ++c)
                             buf[((size_t)(z * ny + y) * nx + x) * comps + c] =
                                 f[(size_t)d.d_idx(x, y, z) * comps + c];
+            src = buf.data(); need = buf.size() * 8;
+        }
+    }
+    else if (n.rfind("ns_", 0) == 0 && d.fluid == 1 && d.cfd_solver == 0) {
+        unsigned nx = d.grid.num[0], ny = d.grid.num[1], nz = d.grid.num[2];
+        size_t nc = (size_t)nx * ny * nz;
+        static thread_local std::vector<double> buf;
+        static thread_local long v;
+        if (n == "ns_nijac_last" || n == "ns_nijac_total" || n == "ns_converged") {
+            v = n == "ns_nijac_last" ? r->nijac_last : n == "ns_nijac_total" ? r->nijac_total : r->ns_converged;
+            src = &v; need = 8;
+        } else if (n == "ns_f_d" || n == "ns_f_p" || n == "ns_f_v" || n == "ns_f_sum") {
+            src = n == "ns_f_d" ? d.dev_ns_f_d : n == "ns_f_p" ? d.dev_ns_f_p
+                  : n == "ns_f_v" ? d.dev_ns_f_v : d.dev_ns_f_sum;
+            need = (size_t)np * 32;
+        } else if (n == "ns_v_face") {
+            size_t nf = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
+            buf.assign(nf * 3, 0.0);
+            size_t q = 0;
+            for (unsigned z = 0; z <= nz; ++z)
+                for (unsigned y = 0; y <= ny; ++y)
+                    for (unsigned x = 0; x <= nx; ++x, ++q) {
+                        unsigned f = d.vidx(x, y, z);
+                        buf[3 * q] = d.dev_ns_v_x[f];
+                        buf[3 * q + 1] = d.dev_ns_v_y[f];
+                        buf[3 * q + 2] = d.dev_ns_v_z[f];
+                    }
+            src = buf.data(); need = buf.size() * 8;
+        } else {
+            const double *f = nullptr;
+            int comps = 1;
+            if (n == "ns_p") f = d.dev_ns_p;
+            else if (n == "ns_phi") f = d.dev_ns_phi;
+            else if (n == "ns_dphi") f = d.dev_ns_dphi;
+            else if (n == "ns_epsilon") f = d.dev_ns_epsilon;
+            else if (n == "ns_norm") f = d.dev_ns_norm;
+            else if (n == "ns_v") { f = (const double *)d.dev_ns_v; comps = 3; }
+            else if (n == "ns_F_pf") { f = (const double *)d.dev_ns_F_pf; comps = 3; }
+            else return -1;
+            buf.assign(nc * comps, 0.0);
+            for (unsigned z = 0; z < nz; ++z)
+                for (unsigned y = 0; y < ny; ++y)
+                    for (unsigned x = 0; x < nx; ++x)
+                        for (int c = 0; c < comps; ++c)
+                            buf[((size_t)(z * ny + y) * nx + x) * comps + c] =
+                                f[(size_t)d.idx(x, y, z) * comps + c];
             src = buf.data(); need = buf.size() * 8;
         }
     }

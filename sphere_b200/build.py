@@ -20,10 +20,11 @@ BUILD = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 # kernels whose results must round exactly like the reference
-NO_FMA = {"dem_kernels.cu", "sort.cu", "darcy.cu", "persistent_fp64.cu", "stats.cu", "render.cu"}
+NO_FMA = {"dem_kernels.cu", "sort.cu", "darcy.cu", "persistent_fp64.cu", "stats.cu", "render.cu",
+          "navierstokes.cu"}
 SOURCES = ["bin_io.cpp", "dem_kernels.cu", "sort.cu", "engine.cu", "darcy.cu", "dem_mixed.cu",
            "noalloc_sort.cu", "engine_persist.cu", "persistent_fp64.cu", "persistent_mixed.cu",
-           "batch.cu", "warmstart.cu", "stats.cu", "render.cu"]
+           "batch.cu", "warmstart.cu", "stats.cu", "render.cu", "navierstokes.cu"]
 
 
 def nvcc() -> str:

@@ -424,6 +424,50 @@ def init_fluid_darcy(d: BinData, mu: float = 8.9e-4, rho_f: float = 1.0e3, p: fl
     d.k_c = k_c
 
 
+def init_fluid_ns(d: BinData, mu: float = 8.9e-4, rho_f: float = 1.0e3, p: float = 0.0,
+                  hydrostatic: bool = False, tolerance: float = 1.0e-3, maxiter: int = 10000,
+                  ndem: int = 1, beta: float = 0.0, theta: float = 1.0, gamma: float = 0.0,
+                  c_v: float = 1.0, bc_bot: int = 0, bc_top: int = 0) -> None:
+    """``sim.initFluid(cfd_solver=0)`` (``python/sphere.py:3395-3470``): the
+    Navier-Stokes arrays on the sorting grid, with the solver settings of
+    ``python/sphere.py:380-411``; ``hydrostatic`` sets the pressures below
+    the top cells to ``p`` plus the weight of the fluid above them."""
+    nx, ny, nz = (int(v) for v in d.num)
+    d.fluid = True
+    d.cfd_solver = 0
+    d.mu = mu
+    d.rho_f = rho_f
+    d.p_f = numpy.full((nx, ny, nz), float(p))
+    if hydrostatic:
+        dz = d.L[2] / nz
+        for iz in range(nz - 1):
+            z = dz * iz + 0.5 * dz
+            depth = d.L[2] - z
+            d.p_f[:, :, iz] = p + (depth - dz) * rho_f * -d.g[2]
+    d.v_f = numpy.zeros((nx, ny, nz, 3))
+    d.phi = numpy.ones((nx, ny, nz))
+    d.dphi = numpy.zeros((nx, ny, nz))
+    d.p_mod_A = d.p_mod_f = d.p_mod_phi = 0.0
+    d.bc_bot = bc_bot
+    d.bc_top = bc_top
+    d.free_slip_bot = d.free_slip_top = 1
+    d.bc_bot_flux = d.bc_top_flux = 0.0
+    d.p_f_constant = numpy.zeros((nx, ny, nz), dtype=numpy.int32)
+    d.ns_gamma = gamma
+    d.ns_theta = theta
+    d.ns_beta = beta
+    d.tolerance = tolerance
+    d.maxiter = maxiter
+    d.ndem = ndem
+    d.c_phi = 1.0
+    d.c_v = c_v
+    d.dt_dem_fac = 1.0
+    d.f_d = numpy.zeros((d.np, 3))
+    d.f_p = numpy.zeros((d.np, 3))
+    d.f_v = numpy.zeros((d.np, 3))
+    d.f_sum = numpy.zeros((d.np, 3))
+
+
 def _fcc_positions(n: int, d_nn: float, z0: float):
     """First n sites of a face-centred cubic lattice with nearest-neighbour
     distance d_nn, filled layer by layer from z0 upward in a square periodic

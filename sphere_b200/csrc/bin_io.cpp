@@ -106,10 +106,9 @@ int parse_bin(const uint8_t *buf, size_t len, int fluid, HostState &s, std::stri
     s.fluid = fluid ? 1 : 0;
     if (fluid) {
         s.cfd_solver = r.i4();
-        if (s.cfd_solver != 1) {
-            err = s.cfd_solver == 0 ? "Navier-Stokes fluid (cfd_solver 0) is not built"
-                                    : "cfd_solver value not understood";
-            return s.cfd_solver == 0 ? ST_UNSUPPORTED : ST_INPUT;
+        if (s.cfd_solver != 0 && s.cfd_solver != 1) {
+            err = "cfd_solver value not understood";
+            return ST_INPUT;
         }
         s.mu = r.f8();
         uint64_t nc = s.ncells();
@@ -121,16 +120,34 @@ int parse_bin(const uint8_t *buf, size_t len, int fluid, HostState &s, std::stri
             s.p_f[i] = r.f8(); s.phi[i] = r.f8(); s.dphi[i] = r.f8();
         }
         s.rho_f = r.f8(); s.p_mod_A = r.f8(); s.p_mod_f = r.f8(); s.p_mod_phi = r.f8();
-        s.bc_xn = r.i4(); s.bc_xp = r.i4(); s.bc_yn = r.i4(); s.bc_yp = r.i4();
-        s.bc_bot = r.i4(); s.bc_top = r.i4();
+        if (s.cfd_solver == 1) {
+            s.bc_xn = r.i4(); s.bc_xp = r.i4(); s.bc_yn = r.i4(); s.bc_yp = r.i4();
+            s.bc_bot = r.i4(); s.bc_top = r.i4();
+        } else {
+            // the Navier-Stokes block has no side conditions and names the
+            // top condition first (src/file_io.cpp:297-298)
+            s.bc_top = r.i4(); s.bc_bot = r.i4();
+        }
         s.free_slip_bot = r.i4(); s.free_slip_top = r.i4();
         s.bc_bot_flux = r.f8(); s.bc_top_flux = r.f8();
         s.p_constant.assign(nc, 0);
         r.take(s.p_constant.data(), 4 * nc);
-        s.tolerance = r.f8(); s.maxiter = r.u4(); s.ndem = r.u4(); s.c_phi = r.f8();
-        s.f_p.assign(n, d4{});
-        for (uint32_t i = 0; i < n; ++i) r.take(&s.f_p[i], 24);
-        s.beta_f = r.f8(); s.k_c = r.f8();
+        if (s.cfd_solver == 0) {
+            // src/file_io.cpp:306-336
+            s.ns_gamma = r.f8(); s.ns_theta = r.f8(); s.ns_beta = r.f8();
+            s.tolerance = r.f8(); s.maxiter = r.u4(); s.ndem = r.u4();
+            s.c_phi = r.f8(); s.c_v = r.f8(); s.dt_dem_fac = r.f8();
+            if ((uint64_t)n * 96 > r.left()) { err = "file truncated in the fluid forces"; return ST_FILE; }
+            for (std::vector<d4> *a : {&s.f_d, &s.f_p, &s.f_v, &s.f_sum}) {
+                a->assign(n, d4{});
+                for (uint32_t i = 0; i < n; ++i) r.take(&(*a)[i], 24);
+            }
+        } else {
+            s.tolerance = r.f8(); s.maxiter = r.u4(); s.ndem = r.u4(); s.c_phi = r.f8();
+            s.f_p.assign(n, d4{});
+            for (uint32_t i = 0; i < n; ++i) r.take(&s.f_p[i], 24);
+            s.beta_f = r.f8(); s.k_c = r.f8();
+        }
     }
     s.color.assign(n, 0);
     r.take(s.color.data(), 4 * (size_t)n);
@@ -202,14 +219,26 @@ std::vector<uint8_t> serialize_bin(const HostState &s)
             w.f8(s.p_f[i]); w.f8(s.phi[i]); w.f8(s.dphi[i]);
         }
         w.f8(s.rho_f); w.f8(s.p_mod_A); w.f8(s.p_mod_f); w.f8(s.p_mod_phi);
-        w.i4(s.bc_xn); w.i4(s.bc_xp); w.i4(s.bc_yn); w.i4(s.bc_yp);
+        if (s.cfd_solver == 1) {
+            w.i4(s.bc_xn); w.i4(s.bc_xp); w.i4(s.bc_yn); w.i4(s.bc_yp);
+        }
+        // bottom first, also for Navier-Stokes, whose reader takes the top
+        // first (src/file_io.cpp:602-603 against 297-298)
         w.i4(s.bc_bot); w.i4(s.bc_top);
         w.i4(s.free_slip_bot); w.i4(s.free_slip_top);
         w.f8(s.bc_bot_flux); w.f8(s.bc_top_flux);
         w.put(s.p_constant.data(), 4 * nc);
-        w.f8(s.tolerance); w.u4(s.maxiter); w.u4(s.ndem); w.f8(s.c_phi);
-        for (uint32_t i = 0; i < n; ++i) w.put(&s.f_p[i], 24);
-        w.f8(s.beta_f); w.f8(s.k_c);
+        if (s.cfd_solver == 0) {
+            w.f8(s.ns_gamma); w.f8(s.ns_theta); w.f8(s.ns_beta);
+            w.f8(s.tolerance); w.u4(s.maxiter); w.u4(s.ndem);
+            w.f8(s.c_phi); w.f8(s.c_v); w.f8(s.dt_dem_fac);
+            for (const std::vector<d4> *a : {&s.f_d, &s.f_p, &s.f_v, &s.f_sum})
+                for (uint32_t i = 0; i < n; ++i) w.put(&(*a)[i], 24);
+        } else {
+            w.f8(s.tolerance); w.u4(s.maxiter); w.u4(s.ndem); w.f8(s.c_phi);
+            for (uint32_t i = 0; i < n; ++i) w.put(&s.f_p[i], 24);
+            w.f8(s.beta_f); w.f8(s.k_c);
+        }
     }
     w.put(s.color.data(), 4 * (size_t)n);
     return w.out;
@@ -277,6 +306,15 @@ int check_values(const HostState &s, std::string &err)
     if (s.k_n <= 0.0) return fail("k_n must be positive");
     if (s.E < 0.0) return fail("E must not be negative");
     if (s.rho <= 0.0) return fail("rho must be positive");
+    if (s.fluid && s.cfd_solver == 0) {
+        // checkValues (src/sphere.cpp:311-317)
+        if (s.rho_f <= 0.0) return fail("fluid density must be positive");
+        // DEM::startTime reads the host pressure at cell (2,2,2)
+        // (device.cu:1564), inside the grid only from 3 cells per axis
+        if (s.num[0] < 3 || s.num[1] < 3 || s.num[2] < 3)
+            return fail("the Navier-Stokes grid needs at least 3 cells per axis");
+        if (s.ndem == 0) return fail("ndem must be positive");
+    }
     if (s.fluid && s.cfd_solver == 1) {
         if (s.rho_f <= 0.0) return fail("fluid density must be positive");
         if (s.mu <= 0.0) return fail("fluid viscosity must be positive");

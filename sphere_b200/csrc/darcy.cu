@@ -830,7 +830,7 @@ static unsigned cells_blocks(const DarcyParams &D) { return ((unsigned)D.nx * D.
 int Engine::darcy_init()
 {
     if (!hs.fluid) return ST_OK;
-    if (hs.cfd_solver != 1) return fail(ST_UNSUPPORTED, "only the Darcy solver (cfd_solver 1) is built");
+    if (hs.cfd_solver == 0) return ns_init();
     if (hs.ndem == 0) return fail(ST_INPUT, "ndem must be positive");
     darcy = new DarcyDev();
     DarcyDev &Dd = *darcy;
@@ -945,6 +945,7 @@ void Engine::darcy_free()
 
 cudaError_t Engine::enqueue_fluid()
 {
+    if (ns) return enqueue_ns();
     if (!darcy) return cudaSuccess;
     DarcyDev &Dd = *darcy;
     const DarcyParams &D = Dd.D;
@@ -1021,6 +1022,7 @@ cudaError_t Engine::enqueue_fluid()
 
 int64_t Engine::darcy_field_bytes(int f) const
 {
+    if (ns) return ns_field_bytes(f);
     if (!darcy) return -1;
     const size_t nc = (size_t)hs.num[0] * hs.num[1] * hs.num[2];
     switch (f) {
@@ -1037,6 +1039,7 @@ int64_t Engine::darcy_field_bytes(int f) const
 
 int Engine::darcy_get(int f, void *dst, size_t bytes)
 {
+    if (ns) return ns_get(f, dst, bytes);
     if (!darcy) return fail(ST_ARG, "no fluid in this run");
     int64_t need = darcy_field_bytes(f);
     if (need < 0) return fail(ST_ARG, "unknown field");
@@ -1096,6 +1099,7 @@ int Engine::darcy_get(int f, void *dst, size_t bytes)
 
 int Engine::darcy_download()
 {
+    if (ns) return ns_download();
     if (!darcy) return ST_OK;
     const size_t nc = hs.ncells();
     int rc;
@@ -1111,7 +1115,7 @@ int Engine::darcy_download()
 
 void Engine::conv_open()
 {
-    if (!darcy) return;
+    if (!darcy && !ns) return;
     std::string f = outdir + "/" + sid + "-conv.log";
     convlog = std::fopen(f.c_str(), "w");
 }
@@ -1127,6 +1131,7 @@ void Engine::conv_close()
 // iteration count is read back for the conv log and the stopping check.
 int Engine::step_with_fluid_log(uint64_t n)
 {
+    if (ns) return ns_step_with_log(n);
     if (!darcy) return step(n);
     int warn = ST_OK;
     for (uint64_t i = 0; i < n; ++i) {

@@ -65,6 +65,7 @@ Engine::~Engine()
 {
     conv_close();
     darcy_free();
+    ns_free();
     persist_free();
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (void *p : allocations) cudaFree(p);
@@ -709,6 +710,7 @@ int Engine::write_bin(const char *path)
     int rc = download_state();
     if (rc < 0) return rc;
     filetimeclock = 0.0;
+    ns_set_host_wall();
     if (darcy) {
         darcy_set_host_wall();
         if ((rc = darcy_sync_wall()) < 0) return rc;
@@ -756,6 +758,9 @@ int Engine::run()
         if (rc > 0) warn = rc;
         t = tt;
         if (output) {
+            // the Navier-Stokes stability check precedes each file
+            // (device.cu:2612-2616)
+            if (ns && ((rc = download_state()) < 0 || (rc = ns_check_stability()) < 0)) return rc;
             hs.step_count += 1;
             std::snprintf(name, sizeof name, "%s/%s.output%05d.bin", outdir.c_str(), sid.c_str(),
                           hs.step_count);

@@ -16,6 +16,7 @@
 namespace sphb {
 
 struct DarcyDev;   // Darcy solver state (darcy.cu)
+struct NSDev;      // Navier-Stokes solver state (navierstokes.cu)
 struct MixedDev;   // mixed-precision state (dem_mixed.cu)
 struct PersistDev; // fused persistent step path (engine_persist.cu)
 
@@ -63,6 +64,7 @@ public:
     std::string err;
 
     DarcyDev *darcy = nullptr;
+    NSDev *ns = nullptr;
     MixedDev *mixed = nullptr;
     PersistDev *persist = nullptr;
     DevState S_view[2]{};         // S_view[v]: buffer view v (S is the current one)
@@ -113,6 +115,16 @@ public:
     int darcy_get(int f, void *dst, size_t bytes);
     int darcy_download();
     int step_with_fluid_log(uint64_t n);
+    // Navier-Stokes (cfd_solver 0, navierstokes.cu)
+    int ns_init();
+    void ns_free();
+    void ns_set_host_wall();
+    cudaError_t enqueue_ns();
+    int64_t ns_field_bytes(int f) const;
+    int ns_get(int f, void *dst, size_t bytes);
+    int ns_download();
+    int ns_check_stability();
+    int ns_step_with_log(uint64_t n);
     void conv_open();
     void conv_close();
 

@@ -47,7 +47,8 @@ struct HostState {
     std::vector<d4> bonds_delta;       // (t.x, t.y, t.z, n)
     std::vector<d4> bonds_omega;
 
-    // fluid (src/datatypes.h:158-190), cfd_solver 1 only
+    // fluid (src/datatypes.h:158-190): Darcy (cfd_solver 1) and
+    // Navier-Stokes (cfd_solver 0) share the grid fields and most settings
     int fluid = 0;
     int32_t cfd_solver = 1;
     double mu = 0;
@@ -63,6 +64,12 @@ struct HostState {
     double c_phi = 1;
     std::vector<d4> f_p;               // np (w unused)
     double beta_f = 4.5e-10, k_c = 4.6e-10;
+    // Navier-Stokes only: smoothing, relaxation, pressure-projection weight,
+    // velocity prefactor, time step factor, and the per-particle drag,
+    // viscous and total interaction forces (f_p above holds the pressure
+    // force)
+    double ns_gamma = 0, ns_theta = 1, ns_beta = 0, c_v = 1, dt_dem_fac = 1;
+    std::vector<d4> f_d, f_v, f_sum;
 
     uint64_t ncells() const { return (uint64_t)num[0] * num[1] * num[2]; }
 };

@@ -24,12 +24,12 @@ FIELDS = [
     "contacts", "delta_t", "distmod", "walls_nx", "walls_mvfd", "walls_acc", "iter",
     "time", "darcy_p", "darcy_phi", "darcy_dphi", "darcy_k", "darcy_v", "darcy_f_p",
     "darcy_iters", "darcy_iters_total", "darcy_iters_exact", "darcy_warm", "bonds", "bonds_delta", "bonds_omega",
-    "velocity_state",
+    "velocity_state", "ns_epsilon", "ns_norm", "ns_v_face", "ns_f_d", "ns_f_v", "ns_f_sum",
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 _VEC4 = {"x", "vel", "angvel", "angpos", "force", "torque", "acc", "angacc", "xyzsum",
          "delta_t", "distmod", "walls_nx", "walls_mvfd", "darcy_f_p", "bonds_delta",
-         "bonds_omega"}
+         "bonds_omega", "ns_f_d", "ns_f_v", "ns_f_sum"}
 _U32 = {"cellid", "index", "cellstart", "cellend", "contacts", "bonds"}
 _I64 = {"iter", "velocity_state", "darcy_iters", "darcy_iters_total", "darcy_iters_exact", "darcy_warm"}
 
@@ -265,7 +265,7 @@ class Engine:
             dtype, shape = numpy.uint32, (nbytes // 4,)
         elif name in _I64:
             dtype, shape = numpy.int64, (nbytes // 8,)
-        elif name == "darcy_v":
+        elif name in ("darcy_v", "ns_v_face"):
             dtype, shape = numpy.float64, (nbytes // 24, 3)
         else:
             dtype, shape = numpy.float64, (nbytes // 8,)
@@ -362,7 +362,7 @@ def _shape_of(name, nbytes):
         return numpy.uint32, (nbytes // 4,)
     if name in _I64:
         return numpy.int64, (nbytes // 8,)
-    if name == "darcy_v":
+    if name in ("darcy_v", "ns_v_face"):
         return numpy.float64, (nbytes // 24, 3)
     return numpy.float64, (nbytes // 8,)
 

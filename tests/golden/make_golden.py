@@ -5,7 +5,8 @@ contactmodels.cuh, cohesion.cuh, integration.cuh), compiled for the host by
 oracle/Makefile into oracle/_ref, run each seeded input below; the input .bin
 and the reference's state after the listed steps are stored as
 <case>.bin + <case>.npz.  Run from the repository root where the reference
-tree is present:  python tests/golden/make_golden.py
+tree is present:  python tests/golden/make_golden.py  (with the argument
+`ns`, only the Navier-Stokes fixture is made).
 """
 import os
 import sys
@@ -58,8 +59,41 @@ def darcy_cases():
     yield "darcy_consolidation", d
 
 
+NS_FIELDS = ("ns_p", "ns_phi", "ns_dphi", "ns_v", "ns_v_face", "ns_epsilon", "ns_norm", "ns_f_d",
+             "ns_f_p", "ns_f_v", "ns_f_sum", "ns_nijac_last", "x", "vel", "force")
+
+
+def ns_cases():
+    """Navier-Stokes (cfd_solver 0): a settling box under a stress-controlled
+    wall in a hydrostatic fluid (navierstokes.cuh, device.cu:1213-1898)."""
+    d = configs.settling_lattice(n=300, seed=16, nx=7, ny=7, nz=7, spacing=0.0195, steps=40)
+    configs.add_top_wall(d, 10e3)
+    d.w_x[0] -= 0.002
+    configs.init_fluid_ns(d, mu=8.9e-4, hydrostatic=True, tolerance=1e-6, maxiter=2000)
+    yield "ns_settling", d
+
+
+def make_ns():
+    for name, d in ns_cases():
+        path = os.path.join(HERE, f"{name}.bin")
+        binfile.write_bin(d, path)
+        ref = O.Reference(path, fluid=True)
+        out = {}
+        for s in (1, 2, 3):
+            ref.step(1)
+            for f in NS_FIELDS:
+                out[f"{f}@{s}"] = ref.get(f)
+        ref.close()
+        numpy.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print(name, "written")
+
+
 def main():
     O.build(ref=True)
+    if sys.argv[1:] == ["ns"]:
+        make_ns()
+        return
+    make_ns()
     for name, d in darcy_cases():
         path = os.path.join(HERE, f"{name}.bin")
         binfile.write_bin(d, path)

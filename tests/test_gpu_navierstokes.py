@@ -1,0 +1,143 @@
+"""The engine's Navier-Stokes solver (cfd_solver 0) against the reference's
+own Navier-Stokes kernels built for the host (oracle/_ref, driven through
+the stage order of DEM::startTime, device.cu:1213-1898) and against the
+committed fixture made from them (tests/golden/ns_settling.*).
+
+The device code keeps the reference's operation order with FMA contraction
+off, but the drag law's pow/exp/log10 come from CUDA's math library on the
+device and glibc's on the host, which may differ in the last bit, and the
+coupled state then drifts by rounding.  Fields are therefore compared to a
+relative tolerance of 1e-9 of each field's largest magnitude; the Jacobi
+iteration counts must match exactly.
+"""
+import os
+
+import numpy
+import pytest
+
+from sphere_b200 import binfile, configs
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-9
+# (engine field, reference field)
+PAIRS = (("darcy_p", "ns_p"), ("darcy_phi", "ns_phi"), ("darcy_dphi", "ns_dphi"),
+         ("darcy_v", "ns_v"), ("ns_v_face", "ns_v_face"), ("ns_epsilon", "ns_epsilon"),
+         ("ns_norm", "ns_norm"), ("ns_f_d", "ns_f_d"), ("darcy_f_p", "ns_f_p"),
+         ("ns_f_v", "ns_f_v"), ("ns_f_sum", "ns_f_sum"), ("x", "x"), ("vel", "vel"),
+         ("force", "force"))
+_PART = {"x", "vel", "force", "darcy_f_p", "ns_f_d", "ns_f_v", "ns_f_sum"}
+
+
+def ns_case(seed, periodic=1, top_wall=False, ndem=1, n=300, maxiter=2000, beta=0.0,
+            bc_bot=0, bc_top=0, p_mod=None, mu=8.9e-4, hydrostatic=True):
+    d = configs.settling_lattice(n=n, seed=seed, nx=7, ny=7, nz=7, spacing=0.0195, steps=40)
+    d.periodic = periodic
+    if top_wall:
+        configs.add_top_wall(d, 10e3)
+        d.w_x[0] -= 0.002
+    configs.init_fluid_ns(d, mu=mu, hydrostatic=hydrostatic, tolerance=1e-6, maxiter=maxiter,
+                          ndem=ndem, beta=beta, bc_bot=bc_bot, bc_top=bc_top)
+    if p_mod is not None:
+        d.p_mod_A, d.p_mod_f = p_mod
+    return d
+
+
+def compare(eng, get_ref, it_ref):
+    bad = {}
+    for a_name, b_name in PAIRS:
+        a = numpy.asarray(eng.get(a_name), dtype=float)
+        b = numpy.asarray(get_ref(b_name), dtype=float)
+        if a_name in _PART:
+            a, b = a.reshape(-1, 4)[:, :3], b.reshape(len(a), -1)[:, :3]
+        a, b = a.ravel(), b.ravel()
+        if a.shape != b.shape:
+            bad[a_name] = f"shape {a.shape} vs {b.shape}"
+            continue
+        scale = max(float(numpy.abs(b).max()), 1e-300)
+        err = float(numpy.abs(a - b).max()) / scale
+        if not err <= RTOL:
+            bad[a_name] = f"relative max error {err:.3e}"
+    it_e = int(eng.get("darcy_iters")[0])
+    if it_e != it_ref:
+        bad["iterations"] = f"{it_e} vs {it_ref}"
+    return bad
+
+
+CASES = {
+    "dirichlet": dict(),
+    "top_wall": dict(top_wall=True),
+    "neumann_bottom": dict(bc_bot=1),
+    "noslip_bottom": dict(bc_bot=2),
+    "neumann_top": dict(bc_top=1),
+    "periodic_x": dict(periodic=2),
+    "pressure_projection": dict(beta=0.5),
+    "ndem2": dict(ndem=2),
+    "top_modulation": dict(p_mod=(200.0, 5.0)),
+    "inviscid": dict(mu=0.0),
+}
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="the reference's host build (oracle/_ref) is absent")
+@pytest.mark.parametrize("name", list(CASES))
+def test_ns_parity(tmp_path, name):
+    from sphere_b200.engine import Engine
+    d = ns_case(61, **CASES[name])
+    path = str(tmp_path / "ns.bin")
+    binfile.write_bin(d, path)
+    ref = O.Reference(path, fluid=True)
+    eng = Engine(path, fluid=True, precision="faithful")
+    for k in range(5):
+        assert eng.step(1) in (0, 1)
+        assert ref.step(1) == 0
+        bad = compare(eng, ref.get, int(ref.get("ns_nijac_last")[0]))
+        assert not bad, f"after step {k + 1}: {bad}"
+    assert int(eng.get("darcy_iters_total")[0]) == int(ref.get("ns_nijac_total")[0])
+    eng.close()
+    ref.close()
+
+
+def test_ns_golden_fixture():
+    """The committed settling fixture (the reference's own kernels built for
+    the host, steps 1-3) reproduced by the device solver."""
+    from sphere_b200.engine import Engine
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    gold = numpy.load(os.path.join(here, "ns_settling.npz"))
+    eng = Engine(os.path.join(here, "ns_settling.bin"), fluid=True, precision="faithful")
+    for step in (1, 2, 3):
+        assert eng.step(1) == 0
+        it = int(gold[f"ns_nijac_last@{step}"].ravel()[0])
+        bad = compare(eng, lambda f: gold[f"{f}@{step}"], it)
+        assert not bad, (step, bad)
+    eng.close()
+
+
+def test_ns_file_roundtrip(tmp_path):
+    """A written output carries the solver's fields in the reference's layout
+    (bottom condition first, which its reader takes as the top one), and the
+    reference writes the same bytes after the same steps."""
+    from sphere_b200.engine import Engine
+    d = ns_case(62, bc_bot=1, bc_top=0)
+    path = str(tmp_path / "ns.bin")
+    binfile.write_bin(d, path)
+    eng = Engine(path, fluid=True, precision="faithful")
+    assert eng.step(2) == 0
+    out = str(tmp_path / "out.bin")
+    eng.write_bin(out)
+    eng.close()
+    back = binfile.read_bin(out, fluid=True)
+    assert back.cfd_solver == 0
+    assert (back.bc_top, back.bc_bot) == (1, 0)
+    if O.ref_available():
+        ref = O.Reference(path, fluid=True)
+        ref.step(2)
+        rout = str(tmp_path / "ref.bin")
+        ref.write_bin(rout)
+        ref.close()
+        a = binfile.read_bin(rout, fluid=True)
+        for name in ("p_f", "phi", "dphi", "v_f", "f_d", "f_p", "f_v", "f_sum"):
+            x, y = numpy.asarray(getattr(back, name)), numpy.asarray(getattr(a, name))
+            scale = max(float(numpy.abs(y).max()), 1e-300)
+            assert float(numpy.abs(x - y).max()) <= RTOL * scale, name

@@ -145,3 +145,20 @@ def test_reference_hertz_model_gives_nan_forces(tmp_path):
     ref = O.Reference(path)
     ref.step(1)
     assert numpy.all(numpy.isfinite(ref.get("x")[:, :3]))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="the reference's host build (oracle/_ref) is absent")
+def test_reference_ns_reproduces_golden_fixture():
+    """The Navier-Stokes fixture under tests/golden is what the reference's
+    own kernels give for its input (the generator is deterministic)."""
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    gold = numpy.load(os.path.join(here, "ns_settling.npz"))
+    ref = O.Reference(os.path.join(here, "ns_settling.bin"), fluid=True)
+    for step in (1, 2, 3):
+        assert ref.step(1) == 0
+        for key in gold.files:
+            name, at = key.split("@")
+            if int(at) == step:
+                assert numpy.array_equal(ref.get(name), gold[key]), key
+    assert int(gold["ns_nijac_last@3"][0]) > 10
+    ref.close()
