@@ -307,6 +307,8 @@ def run_gpu(args):
         out["settle"] = settle_leg(args)
     if args.render:
         out["render"] = render_leg(args, d)
+    if args.ns_steps > 0:
+        out["navier_stokes"] = ns_leg(args)
     return out
 
 
@@ -389,6 +391,58 @@ def batch_leg(args):
         "launch": cfg, "autotuner_trials": len(trials),
         "best_trial_ms_per_step": min(t["ms_per_step"] for t in trials) if trials else None,
     }
+
+
+def ns_leg(args):
+    """Navier-Stokes fluid (cfd_solver 0) coupled to the consolidation
+    packing: the settled N-sphere packing on the 40 x 40 x 80 fluid grid
+    under the 10 kPa wall, water (mu = 8.9e-4 Pa s, rho_f = 1000 kg/m^3) at
+    hydrostatic pressure, the reference's solver defaults (tolerance 1e-3,
+    theta 1, beta 0, ndem 1); faithful FP64.  Per DEM step: the time of the
+    whole step and of its fluid stage, the projection's Jacobi iterations,
+    and the same step of the reference's own kernels built for the host
+    (oracle/_ref, one thread) when it is present."""
+    import tempfile
+    from sphere_b200 import binfile, configs
+    from sphere_b200.engine import Engine
+    d = configs.darcy_benchmark(n=args.particles, seed=SEED, log=log)
+    configs.init_fluid_ns(d, mu=8.9e-4, rho_f=1000.0, hydrostatic=True)
+    steps = args.ns_steps
+    with Engine(d, fluid=True, precision="faithful") as eng:
+        eng.step(3)
+        ms, fluid, iters = [], [], []
+        for _ in range(steps):
+            pr = eng.profile(1)
+            ms.append(pr.step_ms)
+            fluid.append(pr.fluid_ms)
+            iters.append(int(eng.get("darcy_iters")[0]) + 1)
+    out = {
+        "workload": f"Navier-Stokes fluid, N={d.np}, grid {int(d.num[0])}x{int(d.num[1])}x{int(d.num[2])}, "
+                    "water at hydrostatic pressure, tolerance 1e-3, faithful FP64",
+        "dem_steps": steps, "ms_per_dem_step": float(numpy.mean(ms)),
+        "fluid_ms_per_dem_step": float(numpy.mean(fluid)),
+        "jacobi_iters_per_step": float(numpy.mean(iters)),
+        "us_per_jacobi_iteration_upper_bound": 1e3 * float(numpy.sum(fluid)) / max(1, int(numpy.sum(iters))),
+    }
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        if O.ref_available() and args.ns_ref_steps > 0:
+            with tempfile.TemporaryDirectory() as td:
+                path = os.path.join(td, "ns.bin")
+                binfile.write_bin(d, path)
+                ref = O.Reference(path, fluid=True)
+                ref.step(1)
+                t0 = time.perf_counter()
+                ref.step(args.ns_ref_steps)
+                sec = (time.perf_counter() - t0) / args.ns_ref_steps
+                ref.close()
+            out["cpu_reference"] = {"s_per_dem_step": sec, "cores": 1, "kind": "reference",
+                                    "sample": f"{args.ns_ref_steps} DEM steps after the first"}
+            out["speedup_vs_cpu_reference"] = sec / (1e-3 * out["ms_per_dem_step"])
+    except Exception as exc:  # the reference build is optional here
+        out["cpu_reference"] = {"unavailable": str(exc)}
+    return out
 
 
 def render_leg(args, d):
@@ -573,9 +627,13 @@ def main():
                     help="1: time the ray tracer on the headline packing (0 skips it)")
     ap.add_argument("--settle-steps", type=int, default=20000,
                     help="DEM steps of the 10,000-sphere settling leg (0 skips it)")
-    ap.add_argument("--legs", default="shear,darcy,batch,large,settle,render",
+    ap.add_argument("--ns-steps", type=int, default=20,
+                    help="DEM steps of the Navier-Stokes leg (0 skips it)")
+    ap.add_argument("--ns-ref-steps", type=int, default=1,
+                    help="steps of the reference's host build timed beside the Navier-Stokes leg")
+    ap.add_argument("--legs", default="shear,darcy,batch,large,settle,render,ns",
                     help="comma list of legs to run: shear (the headline), darcy, batch, large, "
-                         "settle, render")
+                         "settle, render, ns")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -602,6 +660,8 @@ def main():
             out["settle"] = settle_leg(args)
         if "render" in legs and args.render:
             out["render"] = render_leg(args, workload(args.particles))
+        if "ns" in legs and args.ns_steps > 0:
+            out["navier_stokes"] = ns_leg(args)
         print(json.dumps(out), flush=True)
         return 0
     if "darcy" not in legs:
@@ -614,6 +674,8 @@ def main():
         args.settle_steps = 0
     if "render" not in legs:
         args.render = 0
+    if "ns" not in legs:
+        args.ns_steps = 0
     print(json.dumps(run_gpu(args)), flush=True)
     return 0
 

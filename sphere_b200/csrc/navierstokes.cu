@@ -9,8 +9,9 @@
 // (src/navierstokes.cpp:53-61).  One thread handles one cell (or one face);
 // the projection's Jacobi loop (findNSforcing, ghost nodes,
 // jacobiIterationNS, copyValues, repeated) runs as one cooperative kernel
-// with bounded grid barriers between its phases and the reference's stopping
-// rule (the maximum normalised residual, checked at every 10th iteration)
+// with one bounded grid barrier per iteration (rotating iterate buffers
+// replace the reference's four kernels) and the reference's stopping rule
+// (the maximum normalised residual, checked at every 10th iteration)
 // decided on the device.
 //
 // Where two threads of a reference kernel write one ghost node (a periodic
@@ -23,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -53,7 +55,9 @@ struct NSCtl {
 
 // The fields the Jacobi kernel reads and writes.
 struct NSJacobi {
-    double *eps, *eps_new, *norm, *f, *tmp;
+    double *eps, *b1, *b2;          // the eps field and two rotating iterate buffers
+    const double *eps_new;          // values of the rows the update skips
+    double *norm, *tmp;
     const double *f1, *f2;
 };
 
@@ -61,7 +65,7 @@ struct NSDev {
     NSParams N;
     size_t ng, ngf;                 // padded cell and face counts
     double *p, *v, *v_p, *vp_avg, *d_avg, *F_pf, *phi, *dphi;
-    double *eps, *eps_new, *norm, *f, *f1, *f2, *div_phi_vi_v, *tmp;
+    double *eps, *eps_new, *norm, *f1, *f2, *div_phi_vi_v, *tmp, *b1, *b2;
     double *v_x, *v_y, *v_z, *v_p_x, *v_p_y, *v_p_z, *tau_x, *tau_y, *tau_z;
     double *f_pf;                   // 3 doubles per particle, sorted order (the drag force)
     double4 *f_d, *f_p, *f_v, *f_sum;   // original particle order
@@ -596,68 +600,94 @@ __device__ bool ns_barrier(NSCtl *ctl, unsigned nblocks)
 __device__ __forceinline__ double ldg(const double *p) { return __ldcg(p); }
 
 // The Jacobi loop of the projection step (device.cu:1631-1822) in one
-// cooperative launch.  Per iteration: the forcing from the current interior
-// and the previous iteration's ghost nodes (the reference refreshes the
-// ghosts after the forcing), the ghost nodes, the relaxed Jacobi update with
-// its normalised residual, the copy back; at every 10th iteration the
-// maximum |residual| over the interior decides the stop.
+// cooperative launch with one grid barrier per iteration.
+//
+// The reference's iteration n is four kernels: the forcing from the current
+// interior E_n and the ghost nodes of the previous iterate g(E_n-1) (its
+// ghosts are refreshed after the forcing), the ghost nodes g(E_n), the
+// relaxed Jacobi update from E_n and g(E_n), and the copy back.  Here three
+// padded buffers rotate: iteration n reads E_n with its fresh ghosts from
+// P[n%3] and the previous ghosts from P[(n+2)%3], and writes E_n+1 and its
+// ghost images to P[(n+1)%3], which no block reads during iteration n.  Rows
+// the update skips (Dirichlet boundaries) take E_n+1 from eps_new, as the
+// reference's copy does.  At every 10th iteration the maximum |residual|
+// over the interior decides the stop.  At the end P[0] (the eps field)
+// receives the final interior and the ghosts the reference leaves: those of
+// the final iterate after convergence, those of the last input iterate
+// when maxiter is reached.
 __global__ void __launch_bounds__(256) k_jacobi(NSParams N, NSJacobi J, NSCtl *ctl, unsigned wall0_iz)
 {
     const unsigned nc = (unsigned)N.nx * N.ny * N.nz;
+    const unsigned ng = (unsigned)(N.nx + 2) * (N.ny + 2) * (N.nz + 2);
     const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    const int nx = N.nx, ny = N.ny, nz = N.nz;
     const int zmin = N.bc_bot == 0 ? 1 : 0;
-    const int zmax = N.bc_top == 0 ? N.nz - 2 : N.nz - 1;
+    const int zmax = N.bc_top == 0 ? nz - 2 : nz - 1;
     const double dxdx = N.dx * N.dx, dydy = N.dy * N.dy, dzdz = N.dz * N.dz;
+    const double den = 2.0 * (dxdx * dydy + dxdx * dzdz + dydy * dzdz);
+    // the rotating buffers, selected without a local-memory array
+    auto P = [&](unsigned k) { return k == 0 ? J.eps : k == 1 ? J.b1 : J.b2; };
     __shared__ unsigned long long wmax[8];
     bool ok = true, conv = false;
     long long last = -1;
-    for (unsigned nijac = 0; nijac < N.maxiter; ++nijac) {
-        for (unsigned i = tid; i < nc; i += stride) {
-            int x, y, z;
-            cell_of(N, i, x, y, z);
-            const unsigned c = cix(N, x, y, z);
-            const V3 ge = gradient(N, [&](unsigned q) { return ldg(&J.eps[q]); }, x, y, z);
-            J.f[c] = J.f1[c] - dot3(ge, ld3(J.f2, c));
+    if (N.maxiter > 0) {
+        // P[2] carries the loop's incoming ghost nodes (read by the first
+        // forcing); P[0] gets the fresh ghosts of E_0
+        for (unsigned q = tid; q < ng; q += stride) J.b2[q] = J.eps[q];
+        ok = ns_barrier(ctl, gridDim.x);
+        if (ok) {
+            for (unsigned i = tid; i < nc; i += stride) {
+                int x, y, z;
+                cell_of(N, i, x, y, z);
+                const double val = J.eps[cix(N, x, y, z)];
+                ghost_cell<1>(N, J.eps, x, y, z, &val);
+            }
+            ok = ns_barrier(ctl, gridDim.x);
         }
-        if (!(ok = ns_barrier(ctl, gridDim.x))) break;
-        for (unsigned i = tid; i < nc; i += stride) {
-            int x, y, z;
-            cell_of(N, i, x, y, z);
-            const double val = ldg(&J.eps[cix(N, x, y, z)]);
-            ghost_cell<1>(N, J.eps, x, y, z, &val);
-        }
-        if (!(ok = ns_barrier(ctl, gridDim.x))) break;
-        for (unsigned i = tid; i < nc; i += stride) {
-            int x, y, z;
-            cell_of(N, i, x, y, z);
-            if (z < zmin || z > zmax) continue;
-            const unsigned c = cix(N, x, y, z);
-            const double e_xn = ldg(&J.eps[cix(N, x - 1, y, z)]), e = ldg(&J.eps[c]);
-            const double e_xp = ldg(&J.eps[cix(N, x + 1, y, z)]), e_yn = ldg(&J.eps[cix(N, x, y - 1, z)]);
-            const double e_yp = ldg(&J.eps[cix(N, x, y + 1, z)]), e_zn = ldg(&J.eps[cix(N, x, y, z - 1)]);
-            const double e_zp = ldg(&J.eps[cix(N, x, y, z + 1)]);
-            const double f = ldg(&J.f[c]);
-            double e_new = (-dxdx * dydy * dzdz * f + dydy * dzdz * (e_xn + e_xp) + dxdx * dzdz * (e_yn + e_yp) +
-                            dxdx * dydy * (e_zn + e_zp)) /
-                           (2.0 * (dxdx * dydy + dxdx * dzdz + dydy * dzdz));
-            if ((unsigned)z == wall0_iz) e_new = e;
-            if ((unsigned)z == wall0_iz + 1) e_new = e_zn + N.dp_dz;
-            const double res_norm = (e_new - e) * (e_new - e) / (e_new * e_new + 1.0e-16);
-            const double e_relax = e * (1.0 - N.theta) + e_new * N.theta;
-            J.eps_new[c] = e_relax;
-            J.norm[c] = res_norm;
-        }
-        if (!(ok = ns_barrier(ctl, gridDim.x))) break;
+    }
+    for (unsigned nijac = 0; ok && nijac < N.maxiter; ++nijac) {
+        const double *cur = P(nijac % 3), *prev = P((nijac + 2) % 3);
+        double *next = P((nijac + 1) % 3);
         const bool check = nijac % 10 == 0;
         unsigned long long m = 0;
         for (unsigned i = tid; i < nc; i += stride) {
             int x, y, z;
             cell_of(N, i, x, y, z);
             const unsigned c = cix(N, x, y, z);
-            J.eps[c] = ldg(&J.eps_new[c]);
+            double val, res_norm;
+            if (z >= zmin && z <= zmax) {
+                // findNSforcing: interior from E_n, ghost nodes from g(E_n-1)
+                auto ef = [&](int X, int Y, int Z) {
+                    const bool ghost = X < 0 || X >= nx || Y < 0 || Y >= ny || Z < 0 || Z >= nz;
+                    const unsigned q = cix(N, X, Y, Z);
+                    return ldg(ghost ? &prev[q] : &cur[q]);
+                };
+                const V3 ge = mk3((ef(x + 1, y, z) - ef(x - 1, y, z)) / (2.0 * N.dx),
+                                  (ef(x, y + 1, z) - ef(x, y - 1, z)) / (2.0 * N.dy),
+                                  (ef(x, y, z + 1) - ef(x, y, z - 1)) / (2.0 * N.dz));
+                const double f = J.f1[c] - dot3(ge, ld3(J.f2, c));
+                // jacobiIterationNS from E_n and g(E_n)
+                const double e_xn = ldg(&cur[cix(N, x - 1, y, z)]), e = ldg(&cur[c]);
+                const double e_xp = ldg(&cur[cix(N, x + 1, y, z)]), e_yn = ldg(&cur[cix(N, x, y - 1, z)]);
+                const double e_yp = ldg(&cur[cix(N, x, y + 1, z)]), e_zn = ldg(&cur[cix(N, x, y, z - 1)]);
+                const double e_zp = ldg(&cur[cix(N, x, y, z + 1)]);
+                double e_new = (-dxdx * dydy * dzdz * f + dydy * dzdz * (e_xn + e_xp) +
+                                dxdx * dzdz * (e_yn + e_yp) + dxdx * dydy * (e_zn + e_zp)) /
+                               den;
+                if ((unsigned)z == wall0_iz) e_new = e;
+                if ((unsigned)z == wall0_iz + 1) e_new = e_zn + N.dp_dz;
+                res_norm = (e_new - e) * (e_new - e) / (e_new * e_new + 1.0e-16);
+                val = e * (1.0 - N.theta) + e_new * N.theta;
+                J.norm[c] = res_norm;
+            } else {
+                val = J.eps_new[c];
+                res_norm = J.norm[c];
+            }
+            next[c] = val;
+            ghost_cell<1>(N, next, x, y, z, &val);
             if (check) {
-                const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(ldg(&J.norm[c])));
-                m = b > m ? b : m;
+                const unsigned long long bits = (unsigned long long)__double_as_longlong(fabs(res_norm));
+                m = bits > m ? bits : m;
             }
         }
         const unsigned slot = (nijac / 10) & 1;
@@ -691,51 +721,55 @@ __global__ void __launch_bounds__(256) k_jacobi(NSParams N, NSJacobi J, NSCtl *c
             }
         }
     }
-    if (ok && conv) {
-        for (unsigned i = tid; i < nc; i += stride) {
-            int x, y, z;
-            cell_of(N, i, x, y, z);
-            const double val = ldg(&J.eps[cix(N, x, y, z)]);
-            ghost_cell<1>(N, J.eps, x, y, z, &val);
+    if (ok && last >= 0) {
+        const double *fin = P((unsigned)((last + 1) % 3));
+        const double *gsrc = conv ? fin : P((unsigned)(last % 3));
+        for (unsigned q = tid; q < ng; q += stride) {
+            const int x = (int)(q % (unsigned)(nx + 2)) - 1;
+            const int y = (int)((q / (unsigned)(nx + 2)) % (unsigned)(ny + 2)) - 1;
+            const int z = (int)(q / ((unsigned)(nx + 2) * (unsigned)(ny + 2))) - 1;
+            const bool interior = x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz;
+            const double *src = interior ? fin : gsrc;
+            if (src != J.eps) J.eps[q] = ldg(&src[q]);
         }
-        if (N.gamma > 0.0) {
-            // smoothing<Float>, navierstokes.cuh:2619-2677, reading the whole
-            // field before writing
+    }
+    if (ok && conv && N.gamma > 0.0) {
+        // smoothing<Float>, navierstokes.cuh:2619-2677, reading the whole
+        // field before writing, then the ghost nodes again
+        ok = ns_barrier(ctl, gridDim.x);
+        if (ok) {
+            for (unsigned i = tid; i < nc; i += stride) {
+                int x, y, z;
+                cell_of(N, i, x, y, z);
+                if (z < zmin || z > zmax) continue;
+                const unsigned c = cix(N, x, y, z);
+                const double e_xn = ldg(&J.eps[cix(N, x - 1, y, z)]), e = ldg(&J.eps[c]);
+                const double e_xp = ldg(&J.eps[cix(N, x + 1, y, z)]);
+                const double e_yn = ldg(&J.eps[cix(N, x, y - 1, z)]);
+                const double e_yp = ldg(&J.eps[cix(N, x, y + 1, z)]);
+                const double e_zn = ldg(&J.eps[cix(N, x, y, z - 1)]);
+                const double e_zp = ldg(&J.eps[cix(N, x, y, z + 1)]);
+                const double e_avg = 1.0 / 6.0 * (e_xn + e_xp + e_yn + e_yp + e_zn + e_zp);
+                J.tmp[c] = (1.0 - N.gamma) * e + N.gamma * e_avg;
+            }
             ok = ns_barrier(ctl, gridDim.x);
-            if (ok) {
-                for (unsigned i = tid; i < nc; i += stride) {
-                    int x, y, z;
-                    cell_of(N, i, x, y, z);
-                    if (z < zmin || z > zmax) continue;
-                    const unsigned c = cix(N, x, y, z);
-                    const double e_xn = ldg(&J.eps[cix(N, x - 1, y, z)]), e = ldg(&J.eps[c]);
-                    const double e_xp = ldg(&J.eps[cix(N, x + 1, y, z)]);
-                    const double e_yn = ldg(&J.eps[cix(N, x, y - 1, z)]);
-                    const double e_yp = ldg(&J.eps[cix(N, x, y + 1, z)]);
-                    const double e_zn = ldg(&J.eps[cix(N, x, y, z - 1)]);
-                    const double e_zp = ldg(&J.eps[cix(N, x, y, z + 1)]);
-                    const double e_avg = 1.0 / 6.0 * (e_xn + e_xp + e_yn + e_yp + e_zn + e_zp);
-                    J.tmp[c] = (1.0 - N.gamma) * e + N.gamma * e_avg;
-                }
-                ok = ns_barrier(ctl, gridDim.x);
+        }
+        if (ok) {
+            for (unsigned i = tid; i < nc; i += stride) {
+                int x, y, z;
+                cell_of(N, i, x, y, z);
+                if (z < zmin || z > zmax) continue;
+                const unsigned c = cix(N, x, y, z);
+                J.eps[c] = ldg(&J.tmp[c]);
             }
-            if (ok) {
-                for (unsigned i = tid; i < nc; i += stride) {
-                    int x, y, z;
-                    cell_of(N, i, x, y, z);
-                    if (z < zmin || z > zmax) continue;
-                    const unsigned c = cix(N, x, y, z);
-                    J.eps[c] = ldg(&J.tmp[c]);
-                }
-                ok = ns_barrier(ctl, gridDim.x);
-            }
-            if (ok) {
-                for (unsigned i = tid; i < nc; i += stride) {
-                    int x, y, z;
-                    cell_of(N, i, x, y, z);
-                    const double val = ldg(&J.eps[cix(N, x, y, z)]);
-                    ghost_cell<1>(N, J.eps, x, y, z, &val);
-                }
+            ok = ns_barrier(ctl, gridDim.x);
+        }
+        if (ok) {
+            for (unsigned i = tid; i < nc; i += stride) {
+                int x, y, z;
+                cell_of(N, i, x, y, z);
+                const double val = ldg(&J.eps[cix(N, x, y, z)]);
+                ghost_cell<1>(N, J.eps, x, y, z, &val);
             }
         }
     }
@@ -823,7 +857,8 @@ int Engine::ns_init()
     D.ng = (nx + 2) * (ny + 2) * (nz + 2);
     D.ngf = (nx + 3) * (ny + 3) * (nz + 3);
     const size_t ng = D.ng, ngf = D.ngf;
-    for (double **a : {&D.p, &D.d_avg, &D.phi, &D.dphi, &D.eps, &D.eps_new, &D.norm, &D.f, &D.f1, &D.tmp})
+    for (double **a : {&D.p, &D.d_avg, &D.phi, &D.dphi, &D.eps, &D.eps_new, &D.norm, &D.f1, &D.tmp, &D.b1,
+                       &D.b2})
         *a = dalloc<double>(ng);
     for (double **a : {&D.v, &D.v_p, &D.vp_avg, &D.F_pf, &D.f2, &D.div_phi_vi_v}) *a = dalloc<double>(3 * ng);
     for (double **a : {&D.v_x, &D.v_y, &D.v_z, &D.v_p_x, &D.v_p_y, &D.v_p_z, &D.tau_x, &D.tau_y, &D.tau_z})
@@ -871,8 +906,11 @@ int Engine::ns_init()
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi, 256, 0);
     if (per_sm < 1) return fail(ST_CUDA, "Navier-Stokes Jacobi kernel cannot be resident");
     // two blocks per SM at most: the iteration is barrier bound, and fewer
-    // blocks make each barrier cheaper
-    D.jgrid = std::min<int>(sms * std::min(per_sm, 2), (int)blocks_for(nx * ny * nz));
+    // blocks make each barrier cheaper (SPHB_NS_BLOCKS_PER_SM overrides it
+    // for tuning runs)
+    int bps = 2;
+    if (const char *env = std::getenv("SPHB_NS_BLOCKS_PER_SM")) bps = std::max(1, std::atoi(env));
+    D.jgrid = std::min<int>(sms * std::min(per_sm, bps), (int)blocks_for(nx * ny * nz));
     return ST_OK;
 }
 
@@ -955,7 +993,7 @@ cudaError_t Engine::enqueue_ns()
     k_forcing_const<<<cb, 256, 0, stream>>>(N, D.phi, D.dphi, D.v_p, D.v_p_x, D.v_p_y, D.v_p_z, D.f1, D.f2);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(&D.ctl->max_bits[0], 0, 16, stream)) != cudaSuccess) return e;
-    NSJacobi J{D.eps, D.eps_new, D.norm, D.f, D.tmp, D.f1, D.f2};
+    NSJacobi J{D.eps, D.b1, D.b2, D.eps_new, D.norm, D.tmp, D.f1, D.f2};
     NSParams Nc = N;
     unsigned wall = D.wall0_iz;
     NSCtl *ctl = D.ctl;
