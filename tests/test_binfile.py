@@ -105,3 +105,26 @@ def test_writer_matches_reference_python_writer(tmp_path):
     assert binfile.serialize_bin(d) == ref_bytes
     assert d.E == 7e8 and d.np == n
     assert d.time_dt == pytest.approx(configs.time_step(d), rel=0, abs=0)
+
+
+def test_navier_stokes_block_reads_in_the_c_library(tmp_path):
+    """A Navier-Stokes input passes the library's reader and value checks
+    (no device needed), and a grid under 3 cells per axis is rejected."""
+    from sphere_b200 import binfile, configs
+    from sphere_b200.engine import check_file
+    d = configs.settling_lattice(n=300, seed=61, nx=7, ny=7, nz=7, spacing=0.0195, steps=0)
+    configs.init_fluid_ns(d, hydrostatic=True, bc_bot=1)
+    path = str(tmp_path / "ns.bin")
+    binfile.write_bin(d, path)
+    rc, msg = check_file(path, fluid=True)
+    assert rc == 0, msg
+    back = binfile.read_bin(path, fluid=True)
+    assert back.cfd_solver == 0 and back.bc_bot == 1 and back.bc_top == 0
+    assert numpy.array_equal(back.p_f, d.p_f)
+    small = d.copy()
+    small.num = numpy.array([2, 7, 7], dtype=numpy.uint32)
+    small.L = numpy.array(d.L, dtype=float)
+    configs.init_fluid_ns(small)
+    binfile.write_bin(small, str(tmp_path / "small.bin"))
+    rc, msg = check_file(str(tmp_path / "small.bin"), fluid=True)
+    assert rc != 0 and "3 cells" in msg

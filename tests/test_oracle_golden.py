@@ -10,7 +10,10 @@ import oracle as O
 from helpers import VEC3, bits_equal, diff_report
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(HERE, "*.bin")))
+# the Navier-Stokes fixture has no C restatement to check: it is compared with
+# the reference's host build (test_oracle_reference.py) and the device solver
+CASES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(HERE, "*.bin"))
+               if not os.path.basename(p).startswith("ns_"))
 
 
 @pytest.fixture(scope="module", autouse=True)

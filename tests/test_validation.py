@@ -81,13 +81,9 @@ def test_hertz_model_is_reported_unsupported(tmp_path):
     assert open_status(tmp_path, d)[0] == -7
 
 
-def test_navier_stokes_is_reported_unsupported(tmp_path):
+def test_navier_stokes_fluid_density_is_checked(tmp_path):
+    """checkValues for cfd_solver 0 (src/sphere.cpp:311-317): a fluid density
+    that is not positive fails the value check."""
     d = base()
-    nx, ny, nz = (int(v) for v in d.num)
-    d.fluid = True
-    d.cfd_solver = 0
-    d.mu = 1e-3
-    for a in ("p_f", "phi", "dphi"):
-        setattr(d, a, numpy.zeros((nx, ny, nz)))
-    d.v_f = numpy.zeros((nx, ny, nz, 3))
-    assert open_status(tmp_path, d, fluid=True)[0] == -7
+    configs.init_fluid_ns(d, rho_f=0.0)
+    assert open_status(tmp_path, d, fluid=True)[0] == -3
