@@ -73,7 +73,7 @@ struct NSDev {
     NSCtl *ctl;
     double host_wall0_w;
     unsigned wall0_iz = 10000000u;
-    int jgrid = 0;
+    int jgrid = 0, jthreads = 256;
 };
 
 namespace {
@@ -615,7 +615,8 @@ __device__ __forceinline__ double ldg(const double *p) { return __ldcg(p); }
 // receives the final interior and the ghosts the reference leaves: those of
 // the final iterate after convergence, those of the last input iterate
 // when maxiter is reached.
-__global__ void __launch_bounds__(256) k_jacobi(NSParams N, NSJacobi J, NSCtl *ctl, unsigned wall0_iz)
+template <int NT>
+__global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ctl, unsigned wall0_iz)
 {
     const unsigned nc = (unsigned)N.nx * N.ny * N.nz;
     const unsigned ng = (unsigned)(N.nx + 2) * (N.ny + 2) * (N.nz + 2);
@@ -627,7 +628,7 @@ __global__ void __launch_bounds__(256) k_jacobi(NSParams N, NSJacobi J, NSCtl *c
     const double den = 2.0 * (dxdx * dydy + dxdx * dzdz + dydy * dzdz);
     // the rotating buffers, selected without a local-memory array
     auto P = [&](unsigned k) { return k == 0 ? J.eps : k == 1 ? J.b1 : J.b2; };
-    __shared__ unsigned long long wmax[8];
+    __shared__ unsigned long long wmax[NT / 32];
     bool ok = true, conv = false;
     long long last = -1;
     if (N.maxiter > 0) {
@@ -903,14 +904,23 @@ int Engine::ns_init()
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi, 256, 0);
+    // threads per block of the Jacobi launch: 512 (two blocks per SM hold
+    // one cell per thread on the 40 x 40 x 80 grid; measured 3.1 ms per DEM
+    // step against 3.6 with 256 threads), 256 through SPHB_NS_THREADS
+    D.jthreads = 512;
+    if (const char *env = std::getenv("SPHB_NS_THREADS")) D.jthreads = std::atoi(env) == 256 ? 256 : 512;
+    if (D.jthreads == 512)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi<512>, 512, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi<256>, 256, 0);
     if (per_sm < 1) return fail(ST_CUDA, "Navier-Stokes Jacobi kernel cannot be resident");
     // two blocks per SM at most: the iteration is barrier bound, and fewer
-    // blocks make each barrier cheaper (SPHB_NS_BLOCKS_PER_SM overrides it
-    // for tuning runs)
+    // blocks make each barrier cheaper; three were no faster
+    // (SPHB_NS_BLOCKS_PER_SM overrides it for tuning runs)
     int bps = 2;
     if (const char *env = std::getenv("SPHB_NS_BLOCKS_PER_SM")) bps = std::max(1, std::atoi(env));
-    D.jgrid = std::min<int>(sms * std::min(per_sm, bps), (int)blocks_for(nx * ny * nz));
+    D.jgrid = std::min<int>(sms * std::min(per_sm, bps),
+                            (int)((nx * ny * nz + D.jthreads - 1) / D.jthreads));
     return ST_OK;
 }
 
@@ -998,7 +1008,8 @@ cudaError_t Engine::enqueue_ns()
     unsigned wall = D.wall0_iz;
     NSCtl *ctl = D.ctl;
     void *args[] = {(void *)&Nc, (void *)&J, (void *)&ctl, (void *)&wall};
-    e = cudaLaunchCooperativeKernel((void *)k_jacobi, dim3(D.jgrid), dim3(256), args, 0, stream);
+    e = cudaLaunchCooperativeKernel(D.jthreads == 512 ? (void *)k_jacobi<512> : (void *)k_jacobi<256>,
+                                    dim3(D.jgrid), dim3(D.jthreads), args, 0, stream);
     if (e != cudaSuccess) return e;
     k_update_pressure<<<cb, 256, 0, stream>>>(N, D.eps, D.p);
     k_update_velocity<<<cb, 256, 0, stream>>>(N, D.v_p_x, D.v_p_y, D.v_p_z, D.eps, D.wall0_iz, D.v_x, D.v_y,
