@@ -8,11 +8,11 @@
 // staggered face velocities (nx+3)(ny+3)(nz+3) doubles
 // (src/navierstokes.cpp:53-61).  One thread handles one cell (or one face);
 // the projection's Jacobi loop (findNSforcing, ghost nodes,
-// jacobiIterationNS, copyValues, repeated) runs as one cooperative kernel
-// with one bounded grid barrier per iteration (rotating iterate buffers
-// replace the reference's four kernels) and the reference's stopping rule
-// (the maximum normalised residual, checked at every 10th iteration)
-// decided on the device.
+// jacobiIterationNS, copyValues, repeated) runs as one cooperative kernel:
+// rotating iterate buffers replace the reference's four kernels per
+// iteration, blocks wait (bounded) only for the blocks whose cells they
+// read, and the reference's stopping rule (the maximum normalised residual,
+// checked at every 10th iteration) is decided on the device.
 //
 // Where two threads of a reference kernel write one ghost node (a periodic
 // bottom with a Dirichlet or Neumann top), the reference's result depends on
@@ -50,7 +50,22 @@ struct NSCtl {
     int converged;                  // 1: the last solve met the tolerance
     int err;                        // DERR_TIMEOUT or DERR_NAN
     unsigned barrier_count, barrier_gen;
-    unsigned long long max_bits[2]; // |residual| maxima of alternate checks, ordered bits
+};
+
+// Synchronisation of the cooperative Jacobi kernel (zeroed before each
+// launch).  Block b owns a contiguous range of cells and publishes in
+// done[b] how many iterations it has completed; an iteration reads the
+// previous iterates of the cells within one z layer only (and, with a
+// periodic z boundary, of the far end), so a block waits for the blocks
+// around it instead of the whole grid.  The residual maxima of the check
+// iterations go to a ring of slots and their arrivals are counted, so every
+// block can read a complete maximum.  Each counter has its own 128-byte line.
+constexpr unsigned kNSMaxBlocks = 1024;
+constexpr unsigned kNSChecks = 8;
+struct NSSync {
+    unsigned long long ring[kNSChecks];
+    unsigned arrive[kNSChecks][32];
+    unsigned done[kNSMaxBlocks][32];
 };
 
 // The fields the Jacobi kernel reads and writes.
@@ -71,6 +86,7 @@ struct NSDev {
     double4 *f_d, *f_p, *f_v, *f_sum;   // original particle order
     double *gather;
     NSCtl *ctl;
+    NSSync *sync;
     double host_wall0_w;
     unsigned wall0_iz = 10000000u;
     int jgrid = 0, jthreads = 256;
@@ -600,7 +616,7 @@ __device__ bool ns_barrier(NSCtl *ctl, unsigned nblocks)
 __device__ __forceinline__ double ldg(const double *p) { return __ldcg(p); }
 
 // The Jacobi loop of the projection step (device.cu:1631-1822) in one
-// cooperative launch with one grid barrier per iteration.
+// cooperative launch.
 //
 // The reference's iteration n is four kernels: the forcing from the current
 // interior E_n and the ghost nodes of the previous iterate g(E_n-1) (its
@@ -608,15 +624,44 @@ __device__ __forceinline__ double ldg(const double *p) { return __ldcg(p); }
 // relaxed Jacobi update from E_n and g(E_n), and the copy back.  Here three
 // padded buffers rotate: iteration n reads E_n with its fresh ghosts from
 // P[n%3] and the previous ghosts from P[(n+2)%3], and writes E_n+1 and its
-// ghost images to P[(n+1)%3], which no block reads during iteration n.  Rows
-// the update skips (Dirichlet boundaries) take E_n+1 from eps_new, as the
-// reference's copy does.  At every 10th iteration the maximum |residual|
-// over the interior decides the stop.  At the end P[0] (the eps field)
-// receives the final interior and the ghosts the reference leaves: those of
-// the final iterate after convergence, those of the last input iterate
-// when maxiter is reached.
+// ghost images to P[(n+1)%3].  Rows the update skips (Dirichlet boundaries)
+// take E_n+1 from eps_new, as the reference's copy does.
+//
+// Block b updates the cells [b*chunk, (b+1)*chunk).  Before iteration n it
+// waits until the blocks whose cells lie within reach (one z layer, one row
+// and one cell: the stencil and the ghost nodes the cells write; the whole
+// grid with a periodic z boundary) have completed iteration n-1.  That makes
+// their part of E_n visible, and since those are the only blocks that read
+// this block's cells, none of them still reads the buffer iteration n
+// overwrites.  At every 10th iteration each block adds its maximum
+// |residual| to a slot and its arrival to a counter; the stop is decided at
+// the start of the next iteration from the complete maximum.  At the end
+// P[0] (the eps field) receives the final interior and the ghosts the
+// reference leaves: those of the final iterate after convergence, those of
+// the last input iterate when maxiter is reached.
+
+// Waits (thread-wise, bounded) until *p >= target with acquire semantics;
+// records DERR_TIMEOUT after ~2^22 polls or stops when another block has
+// flagged an error.
+__device__ __forceinline__ bool ns_wait_ge(const unsigned *p, unsigned target, NSCtl *ctl)
+{
+    unsigned spins = 0, nap = 16;
+    for (;;) {
+        unsigned v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        if (v >= target) return true;
+        if (++spins > (1u << 22)) {
+            atomicCAS(&ctl->err, 0, (int)DERR_TIMEOUT);
+            return false;
+        }
+        if (*(volatile int *)&ctl->err != 0) return false;
+        __nanosleep(nap);
+        if (nap < 128) nap <<= 1;
+    }
+}
+
 template <int NT>
-__global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ctl, unsigned wall0_iz)
+__global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ctl, NSSync *S, unsigned wall0_iz)
 {
     const unsigned nc = (unsigned)N.nx * N.ny * N.nz;
     const unsigned ng = (unsigned)(N.nx + 2) * (N.ny + 2) * (N.nz + 2);
@@ -646,12 +691,59 @@ __global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ct
             ok = ns_barrier(ctl, gridDim.x);
         }
     }
+    // this block's cells and the blocks whose cells its iteration reads
+    const unsigned G = gridDim.x, b = blockIdx.x;
+    const unsigned chunk = (nc + G - 1) / G;
+    const unsigned lo = min(nc, b * chunk), hi = min(nc, lo + chunk);
+    const bool zwrap = N.bc_bot == 2 || N.bc_top == 2;
+    const unsigned reach = zwrap ? nc : (unsigned)nx * ny + (unsigned)nx + 1u;
+    const unsigned nb_lo = lo > reach ? (lo - reach) / chunk : 0u;
+    const unsigned nb_hi = min(G - 1u, (hi + reach) / chunk);
+    __shared__ int s_state;   // 0 continue, 1 converged, 2 stop (error)
+    if (threadIdx.x == 0) s_state = 0;
+    __syncthreads();
+    // the stop rule of check iteration c (thread 0): every block's maximum
+    auto decide = [&](unsigned c) {
+        const unsigned k = c / 10u;
+        if (!ns_wait_ge(&S->arrive[k % kNSChecks][0], G, ctl)) {
+            s_state = 2;
+            return;
+        }
+        const unsigned long long mb = __ldcg(&S->ring[k % kNSChecks]);
+        if (b == 0) {
+            // every block has decided the checks before k
+            S->ring[(k + kNSChecks / 2) % kNSChecks] = 0ull;
+            if (k >= 2) S->arrive[(k - 2) % kNSChecks][0] = 0u;
+        }
+        if (mb > 0x7ff0000000000000ull) {
+            // a NaN residual: maxNormResNS stops the run (navierstokes.cpp:283-300)
+            atomicCAS(&ctl->err, 0, (int)DERR_NAN);
+            s_state = 2;
+        } else if (__longlong_as_double((long long)mb) < N.tolerance) {
+            s_state = 1;
+        }
+    };
     for (unsigned nijac = 0; ok && nijac < N.maxiter; ++nijac) {
+        if (threadIdx.x < 32 && nijac > 0) {
+            if (threadIdx.x == 0 && (nijac - 1u) % 10u == 0u) decide(nijac - 1u);
+            __syncwarp();
+            if (s_state == 0) {
+                // the lanes of warp 0 watch the neighbours in parallel
+                bool okw = true;
+                for (unsigned q = nb_lo + threadIdx.x; q <= nb_hi; q += 32)
+                    if (q != b && !ns_wait_ge(&S->done[q][0], nijac, ctl)) okw = false;
+                if (!__all_sync(0xffffffffu, okw) && threadIdx.x == 0) s_state = 2;
+            }
+        }
+        // the acquire loads above and this barrier make the neighbours'
+        // cells visible to the whole block
+        __syncthreads();
+        if (s_state != 0) break;
         const double *cur = P(nijac % 3), *prev = P((nijac + 2) % 3);
         double *next = P((nijac + 1) % 3);
         const bool check = nijac % 10 == 0;
         unsigned long long m = 0;
-        for (unsigned i = tid; i < nc; i += stride) {
+        for (unsigned i = lo + threadIdx.x; i < hi; i += blockDim.x) {
             int x, y, z;
             cell_of(N, i, x, y, z);
             const unsigned c = cix(N, x, y, z);
@@ -691,37 +783,37 @@ __global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ct
                 m = bits > m ? bits : m;
             }
         }
-        const unsigned slot = (nijac / 10) & 1;
         if (check) {
             for (int o = 16; o > 0; o >>= 1) {
                 const unsigned long long q = __shfl_down_sync(0xffffffffu, m, o);
                 m = q > m ? q : m;
             }
             if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
-            __syncthreads();
-            if (threadIdx.x == 0) {
+        }
+        // the barrier orders every thread's cell stores before thread 0's
+        // release (cumulative at GPU scope), so the neighbours may go on
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(&S->done[b][0]), "r"(nijac + 1u) : "memory");
+            if (check) {
                 unsigned long long bm = 0;
-                for (unsigned w = 0; w < blockDim.x / 32; ++w) bm = wmax[w] > bm ? wmax[w] : bm;
-                atomicMax(&ctl->max_bits[slot], bm);
+                for (unsigned w = 0; w < NT / 32; ++w) bm = wmax[w] > bm ? wmax[w] : bm;
+                const unsigned k = nijac / 10u;
+                atomicMax(&S->ring[k % kNSChecks], bm);
+                asm volatile("red.release.gpu.global.add.u32 [%0], 1;" :: "l"(&S->arrive[k % kNSChecks][0]) : "memory");
             }
         }
-        if (!(ok = ns_barrier(ctl, gridDim.x))) break;
         last = nijac;
-        if (check) {
-            const unsigned long long mb = *((volatile unsigned long long *)&ctl->max_bits[slot]);
-            if (blockIdx.x == 0 && threadIdx.x == 0) ctl->max_bits[slot ^ 1u] = 0ull;
-            if (mb > 0x7ff0000000000000ull) {
-                // a NaN residual: maxNormResNS stops the run (navierstokes.cpp:283-300)
-                if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(&ctl->err, 0, (int)DERR_NAN);
-                ok = false;
-                break;
-            }
-            if (__longlong_as_double((long long)mb) < N.tolerance) {
-                conv = true;
-                break;
-            }
-        }
     }
+    // the last iteration's check, when the loop ran to maxiter
+    if (threadIdx.x == 0 && s_state == 0 && last >= 0 && last + 1 == (long long)N.maxiter &&
+        (unsigned)last % 10u == 0u)
+        decide((unsigned)last);
+    __syncthreads();
+    if (s_state == 2) ok = false;
+    conv = s_state == 1;
+    // every block's cells before the final copy
+    if (ok && last >= 0) ok = ns_barrier(ctl, gridDim.x);
     if (ok && last >= 0) {
         const double *fin = P((unsigned)((last + 1) % 3));
         const double *gsrc = conv ? fin : P((unsigned)(last % 3));
@@ -868,6 +960,7 @@ int Engine::ns_init()
     for (double4 **a : {&D.f_d, &D.f_p, &D.f_v, &D.f_sum}) *a = dalloc<double4>(hs.np);
     D.gather = dalloc<double>(3 * (nx + 1) * (ny + 1) * (nz + 1));
     D.ctl = dalloc<NSCtl>(1);
+    D.sync = dalloc<NSSync>(1);
     if (alloc_failed) return fail(ST_CUDA, "device allocation failed (Navier-Stokes)");
     // interior cells from the file; the ghost nodes start at zero
     auto cidx_h = [&](size_t x, size_t y, size_t z) {
@@ -904,23 +997,22 @@ int Engine::ns_init()
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // threads per block of the Jacobi launch: 512 (two blocks per SM hold
-    // one cell per thread on the 40 x 40 x 80 grid; measured 3.1 ms per DEM
-    // step against 3.6 with 256 threads), 256 through SPHB_NS_THREADS
-    D.jthreads = 512;
-    if (const char *env = std::getenv("SPHB_NS_THREADS")) D.jthreads = std::atoi(env) == 256 ? 256 : 512;
+    // threads per block of the Jacobi launch: 256, four blocks per SM (one
+    // cell per thread on the 40 x 40 x 80 grid; measured 2.5 ms per DEM step
+    // against 2.7 with two blocks of 512 and 3.2 with two of 256);
+    // SPHB_NS_THREADS=512 and SPHB_NS_BLOCKS_PER_SM override them for tuning
+    D.jthreads = 256;
+    if (const char *env = std::getenv("SPHB_NS_THREADS")) D.jthreads = std::atoi(env) == 512 ? 512 : 256;
     if (D.jthreads == 512)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi<512>, 512, 0);
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jacobi<256>, 256, 0);
     if (per_sm < 1) return fail(ST_CUDA, "Navier-Stokes Jacobi kernel cannot be resident");
-    // two blocks per SM at most: the iteration is barrier bound, and fewer
-    // blocks make each barrier cheaper; three were no faster
-    // (SPHB_NS_BLOCKS_PER_SM overrides it for tuning runs)
-    int bps = 2;
+    int bps = 4;
     if (const char *env = std::getenv("SPHB_NS_BLOCKS_PER_SM")) bps = std::max(1, std::atoi(env));
     D.jgrid = std::min<int>(sms * std::min(per_sm, bps),
                             (int)((nx * ny * nz + D.jthreads - 1) / D.jthreads));
+    D.jgrid = std::min<int>(D.jgrid, (int)kNSMaxBlocks);
     return ST_OK;
 }
 
@@ -1002,12 +1094,13 @@ cudaError_t Engine::enqueue_ns()
     }
     k_forcing_const<<<cb, 256, 0, stream>>>(N, D.phi, D.dphi, D.v_p, D.v_p_x, D.v_p_y, D.v_p_z, D.f1, D.f2);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(&D.ctl->max_bits[0], 0, 16, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(D.sync, 0, sizeof(NSSync), stream)) != cudaSuccess) return e;
     NSJacobi J{D.eps, D.b1, D.b2, D.eps_new, D.norm, D.tmp, D.f1, D.f2};
     NSParams Nc = N;
     unsigned wall = D.wall0_iz;
     NSCtl *ctl = D.ctl;
-    void *args[] = {(void *)&Nc, (void *)&J, (void *)&ctl, (void *)&wall};
+    NSSync *sync = D.sync;
+    void *args[] = {(void *)&Nc, (void *)&J, (void *)&ctl, (void *)&sync, (void *)&wall};
     e = cudaLaunchCooperativeKernel(D.jthreads == 512 ? (void *)k_jacobi<512> : (void *)k_jacobi<256>,
                                     dim3(D.jgrid), dim3(D.jthreads), args, 0, stream);
     if (e != cudaSuccess) return e;
