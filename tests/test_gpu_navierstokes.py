@@ -32,8 +32,14 @@ _PART = {"x", "vel", "force", "darcy_f_p", "ns_f_d", "ns_f_v", "ns_f_sum"}
 
 
 def ns_case(seed, periodic=1, top_wall=False, ndem=1, n=300, maxiter=2000, beta=0.0,
-            bc_bot=0, bc_top=0, p_mod=None, mu=8.9e-4, hydrostatic=True):
-    d = configs.settling_lattice(n=n, seed=seed, nx=7, ny=7, nz=7, spacing=0.0195, steps=40)
+            bc_bot=0, bc_top=0, p_mod=None, mu=8.9e-4, hydrostatic=True, lattice=(7, 7, 7),
+            tall=1):
+    d = configs.settling_lattice(n=n, seed=seed, nx=lattice[0], ny=lattice[1], nz=lattice[2],
+                                 spacing=0.0195, steps=40)
+    if tall > 1:
+        # the same cells, `tall` times as many layers (fluid above the packing)
+        d.L = numpy.array([d.L[0], d.L[1], d.L[2] * tall])
+        d.num = numpy.array([d.num[0], d.num[1], d.num[2] * tall], dtype=numpy.uint32)
     d.periodic = periodic
     if top_wall:
         configs.add_top_wall(d, 10e3)
@@ -77,6 +83,12 @@ CASES = {
     "ndem2": dict(ndem=2),
     "top_modulation": dict(p_mod=(200.0, 5.0)),
     "inviscid": dict(mu=0.0),
+    # an 11 x 11 x 22 grid: the Jacobi launch spans several blocks that
+    # wait for their z neighbours (or, with the periodic z ghosts of
+    # bc_bot 2, for all blocks)
+    "multiblock": dict(n=1500, lattice=(12, 12, 11), tall=2),
+    "multiblock_wall": dict(n=1500, lattice=(12, 12, 11), tall=2, top_wall=True),
+    "multiblock_zwrap": dict(n=1500, lattice=(12, 12, 11), tall=2, bc_bot=2),
 }
 
 
