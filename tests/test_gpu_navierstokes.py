@@ -221,3 +221,23 @@ def test_ns_smoothing_runs(tmp_path):
     assert numpy.isfinite(eng.get("ns_epsilon")).all()
     assert numpy.isfinite(eng.get("darcy_v")).all()
     eng.close()
+
+
+def test_ns_with_mixed_precision_contacts(tmp_path):
+    """The fluid stage is FP64 in every precision; with mixed-precision
+    contacts the coupled run stays within the mixed mode's force tolerance
+    of the faithful one over a few steps, with the same iteration counts."""
+    from sphere_b200.engine import Engine
+    d = ns_case(66, top_wall=True)
+    path = str(tmp_path / "m.bin")
+    binfile.write_bin(d, path)
+    a = Engine(path, fluid=True, precision="faithful")
+    b = Engine(path, fluid=True, precision="mixed")
+    for _ in range(5):
+        assert a.step(1) == 0 and b.step(1) == 0
+        assert int(a.get("darcy_iters")[0]) == int(b.get("darcy_iters")[0])
+    for name in ("darcy_p", "darcy_v", "ns_f_d"):
+        x, y = numpy.asarray(b.get(name), dtype=float), numpy.asarray(a.get(name), dtype=float)
+        assert numpy.linalg.norm(x - y) <= 1e-5 * numpy.linalg.norm(y), name
+    a.close()
+    b.close()
