@@ -997,9 +997,10 @@ int Engine::ns_init()
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // threads per block of the Jacobi launch: 256, four blocks per SM (one
-    // cell per thread on the 40 x 40 x 80 grid; measured 2.5 ms per DEM step
-    // against 2.7 with two blocks of 512 and 3.2 with two of 256);
+    // threads per block of the Jacobi launch: 256, up to four blocks per SM
+    // and one cell per thread (500 blocks on the 40 x 40 x 80 grid; measured
+    // 2.5 ms per DEM step against 2.7 with 250 blocks of 512 and 3.2 with 296
+    // of 256);
     // SPHB_NS_THREADS=512 and SPHB_NS_BLOCKS_PER_SM override them for tuning
     D.jthreads = 256;
     if (const char *env = std::getenv("SPHB_NS_THREADS")) D.jthreads = std::atoi(env) == 512 ? 512 : 256;
