@@ -241,3 +241,52 @@ def test_ns_with_mixed_precision_contacts(tmp_path):
         assert numpy.linalg.norm(x - y) <= 1e-5 * numpy.linalg.norm(y), name
     a.close()
     b.close()
+
+
+def _cfd_box(ptop=None):
+    """The reference's tests/cfd_tests.py set-up: one sphere (r = 0.05 m) in
+    a 1 m box, fluid with mu = 0 and p = 0, ten time steps, a file each."""
+    from sphere_b200.binfile import BinData
+    d = BinData()
+    configs._particles(d, 1)
+    d.radius = numpy.array([0.05])
+    d.x[0, :] = [0.5, 0.5, 0.5]
+    configs.default_params(d)
+    configs.grid_for(d, L=[1.0, 1.0, 1.0])
+    configs.init_temporal(d, total=0.2, file_dt=0.01)
+    d.time_file_dt = d.time_dt * 0.99
+    d.time_total = d.time_dt * 10
+    configs.init_fluid_ns(d, mu=0.0)
+    if ptop is not None:
+        d.p_f[:, :, -1] = ptop
+    return d
+
+
+def _run_files(tmp_path, d, sid):
+    from sphere_b200.engine import Engine
+    path = str(tmp_path / f"{sid}.bin")
+    binfile.write_bin(d, path)
+    out = tmp_path / sid
+    out.mkdir()
+    eng = Engine(path, fluid=True, output_dir=str(out))
+    assert eng.run() == 0
+    eng.close()
+    last = sorted(p for p in os.listdir(out) if ".output" in p)[-1]
+    conv = numpy.loadtxt(str(out / f"{sid}-conv.log"), ndmin=2)
+    return binfile.read_bin(str(out / last), fluid=True), conv
+
+
+def test_ns_reference_cfd_invariants(tmp_path):
+    """The checks of the reference's tests/cfd_tests.py (Dirichlet
+    boundaries) through run(), its files and its conv log: a fluid at rest
+    stays at rest with no iterations; a raised top pressure relaxes to a
+    linear profile (within 0.1 of it) with downward flow only."""
+    py, conv = _run_files(tmp_path, _cfd_box(), "rest")
+    assert numpy.array_equal(py.p_f, numpy.zeros(py.p_f.shape))
+    assert conv[:, 1].sum() == 0.0
+    assert (numpy.abs(py.v_f) < 1.0e-6).all()
+    d = _cfd_box(ptop=1.1)
+    py, conv = _run_files(tmp_path, d, "grad")
+    ideal = numpy.linspace(d.p_f[0, 0, 0], d.p_f[0, 0, -1], int(d.num[2]))
+    assert numpy.abs(ideal - py.p_f[0, 0, :]).max() < 1.0e-1
+    assert (py.v_f[:, :, :, 2] < 0.0).all() and (py.v_f[:, :, :, 0:1] < 1.0e-7).all()
