@@ -290,3 +290,40 @@ def test_ns_reference_cfd_invariants(tmp_path):
     ideal = numpy.linspace(d.p_f[0, 0, 0], d.p_f[0, 0, -1], int(d.num[2]))
     assert numpy.abs(ideal - py.p_f[0, 0, :]).max() < 1.0e-1
     assert (py.v_f[:, :, :, 2] < 0.0).all() and (py.v_f[:, :, :, 0:1] < 1.0e-7).all()
+
+
+def _one_fluid_box(positions, ndem=1, g=None, p_bot=None, p_top=None, total=0.01, file_dt=0.001):
+    """The reference's tests/fluid_particle_interaction.py set-up: a 1 m box
+    on 0.1 m cells, water (initFluid's defaults), particles of the fluid's
+    density (r = 0.05 m)."""
+    from sphere_b200.binfile import BinData
+    d = BinData()
+    configs._particles(d, len(positions))
+    d.radius = numpy.full(len(positions), 0.05)
+    d.x[:, :] = numpy.asarray(positions, dtype=float)
+    configs.default_params(d, rho=1000.0)
+    if g is not None:
+        d.g = numpy.asarray(g, dtype=float)
+    configs.grid_for(d, L=[1.0, 1.0, 1.0], dx=0.1)
+    configs.init_temporal(d, total=total, file_dt=file_dt)
+    configs.init_fluid_ns(d, ndem=ndem)
+    if p_bot is not None:
+        d.p_f[:, :, 0] = p_bot
+    if p_top is not None:
+        d.p_f[:, :, -1] = p_top
+    return d
+
+
+def test_ns_reference_fluid_particle_interaction(tmp_path):
+    """The checks of the reference's tests/fluid_particle_interaction.py: a
+    pressure gradient (10 Pa at the bottom, 1 Pa at the top) lifts a
+    neutrally buoyant sphere; a fluid driven along x by gravity moves along
+    x everywhere and drags the spheres with it."""
+    d = _one_fluid_box([[0.5, 0.5, 0.5]], ndem=100, p_bot=10.0, p_top=1.0)
+    py, _ = _run_files(tmp_path, d, "lift")
+    assert py.vel[0, 2] > 0.0
+    d = _one_fluid_box([[0.5, 0.5, 0.75], [0.5, 0.5, 0.50], [0.5, 0.5, 0.25]], g=[10.0, 0.0, 0.0],
+                       total=0.0001, file_dt=0.00001)
+    py, _ = _run_files(tmp_path, d, "drag")
+    assert (py.v_f[:, :, :, 0] > 0.0).all()
+    assert (py.vel[:, 0] > 0.0).all()
