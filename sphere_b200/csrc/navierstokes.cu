@@ -1240,6 +1240,10 @@ int Engine::ns_step_with_log(uint64_t n)
         if (e != cudaSuccess) return cuda_fail(e, "step");
         advance_host_clock(1);
         warmed = true;
+        // steps without a projection (ndem > 1) need no read-back; device
+        // errors stop the kernels and are reported at the next projection
+        // or at the end of the call
+        if ((it % (int64_t)ns->N.ndem) != 0 && i + 1 < n) continue;
         NSCtl c;
         e = cudaMemcpyAsync(&c, ns->ctl, sizeof c, cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
