@@ -114,8 +114,19 @@ class ClockSampler:
 
 
 def workload(n):
+    """The dense-shear workload.  At the benchmark size the settled packing
+    is the packaged fixture (sphere_b200/data), so neither arm settles
+    anything and the CPU reference arm never touches the GPU engine."""
     from sphere_b200 import configs
     return configs.shear_benchmark(n=n, seed=SEED, log=log)
+
+
+def workload_config(n):
+    """The `config` of both arms' JSON lines: the same workload and the same
+    DEM steps per benchmark step."""
+    return {"workload": f"dense dry shear, N={n}, radii U(0.008,0.012) m, E=7e8 Pa, "
+                        f"mu=0.5, sigma0=20 kPa, shear 1e-4 m/s, periodic x/y",
+            "dem_steps_per_step": INTERVAL}
 
 
 def mean_contacts(eng, n):
@@ -163,17 +174,33 @@ def shear_report(d, eng, info):
             "dilation_mean_diameters": (w_x - float(d.w_x[0])) / d_bar}
 
 
-def force_error(d):
-    """Normwise relative force error of the mixed mode against FP64 after
-    one step from the same state: ||F_mixed - F_fp64|| / ||F_fp64||."""
+HISTORY_STEPS = 1000
+
+
+def force_error(d, history_steps=HISTORY_STEPS):
+    """Normwise relative force error of the mixed mode against FP64,
+    ||F_mixed - F_fp64|| / ||F_fp64||, after one step from the same sheared
+    state: the workload is first sheared for history_steps FP64 steps, so the
+    contacts carry developed tangential displacements (the FP32 history path
+    of the mixed contact law contributes); positions, velocities, walls,
+    contact rows and histories are then copied into fresh FP64 and mixed
+    engines, which take one step each.  Returns (error, mean occupied slots
+    with a non-zero history per particle)."""
     from sphere_b200.engine import Engine
+    fields = ("x", "vel", "angvel", "walls_nx", "walls_mvfd", "contacts", "delta_t")
+    with Engine(d, precision="fp64") as e:
+        e.step(history_steps)
+        state = {f: e.get(f) for f in fields}
     out = {}
     for prec in ("fp64", "mixed"):
         with Engine(d, precision=prec) as e:
+            for f in fields:
+                e.set(f, state[f])
             e.step(1)
             out[prec] = e.get("force")[:, :3]
     a, b = out["mixed"], out["fp64"]
-    return float(numpy.linalg.norm(a - b) / numpy.linalg.norm(b))
+    live = float((numpy.abs(state["delta_t"][:, :3]).sum(axis=1) > 0).sum()) / d.np
+    return float(numpy.linalg.norm(a - b) / numpy.linalg.norm(b)), live
 
 
 def run_gpu(args):
@@ -261,15 +288,10 @@ def run_gpu(args):
         "vs_baseline": None,
         "dtype": {"faithful": "f64", "fp64": "f64", "mixed": "f32+f64"}[precision],
         "data": "synthetic (seeded settled packing)",
-        "config": {
-            "workload": f"dense dry shear, N={n}, radii U(0.008,0.012) m, E=7e8 Pa, "
-                        f"mu=0.5, sigma0=20 kPa, shear 1e-4 m/s, periodic x/y",
-            "dem_steps_per_step": INTERVAL,
-            "precision": precision,
-            "integrator": "TY3",
-            "mean_contacts_per_particle": zbar,
-            "l2": "flushed between timed steps (256 MB write)",
-        },
+        "config": workload_config(n),
+        "engine": {"precision": precision, "integrator": "TY3",
+                   "mean_contacts_per_particle": zbar,
+                   "l2": "flushed between timed steps (256 MB write)"},
         "e2e": {"value": e2e_value, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": 3 * 32 * n, "d2h_bytes_per_step": 5 * 32 * n},
         "gpu_launches": timed_launches,
@@ -294,7 +316,10 @@ def run_gpu(args):
         out["fp64_plain"] = {"value": plain["value"], "ms_per_step": plain["ms_per_step"],
                              "speedup_of_headline": value / plain["value"]}
     if precision == "mixed":
-        out["force_rel_err_vs_fp64"] = force_error(d)
+        err, live = force_error(d)
+        out["force_rel_err_vs_fp64"] = err
+        out["force_err_state"] = {"history_steps": HISTORY_STEPS,
+                                  "slots_with_tangential_history_per_particle": live}
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(d, sample_steps=args.cpu_steps)
     if args.darcy_steps > 0:
@@ -573,6 +598,9 @@ def run_reference(args):
         path = os.path.join(td, "w.bin")
         binfile.write_bin(d, path)
         orc = O.Oracle(path, precision="faithful")
+        # warm-up steps: one DEM step each (the CPU code has no state a
+        # longer warm-up would prepare); timed steps: INTERVAL DEM steps
+        # each, as in the engine arm
         for _ in range(args.warmup):
             orc.step(1)
         for _ in range(args.steps):
@@ -586,15 +614,17 @@ def run_reference(args):
     total = float(numpy.sum(times))
     value = n * args.ref_sample * args.steps / total
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    sample = f"{args.ref_sample} DEM steps of the N={n} workload per benchmark step"
+    sample = (f"{args.ref_sample} DEM steps of the N={n} workload per benchmark step: the oracle "
+              f"(a C restatement of the reference's FP64 step, pinned bit-exact against the "
+              f"reference's own kernels built for the host), OpenMP on {cores} threads")
+    cfg = workload_config(n)
+    cfg["dem_steps_per_step"] = args.ref_sample
     return {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded settled packing)",
-        "config": {"workload": f"dense dry shear, N={n}, radii U(0.008,0.012) m, E=7e8 Pa, "
-                               f"mu=0.5, sigma0=20 kPa, shear 1e-4 m/s, periodic x/y",
-                   "dem_steps_per_step": args.ref_sample},
+        "config": cfg,
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
                          "kind": "port", "sample": sample},
@@ -612,7 +642,8 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["faithful", "fp64", "mixed"])
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--ref-sample", type=int, default=2)
+    ap.add_argument("--ref-sample", type=int, default=INTERVAL,
+                    help="DEM steps per benchmark step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--darcy-steps", type=int, default=200,
                     help="fluid steps per arm of the Darcy leg (0 skips it)")

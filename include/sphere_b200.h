@@ -47,6 +47,12 @@ enum {
 };
 
 typedef struct sph_opts {
+    size_t struct_size;   /* sizeof(sph_opts) as the caller compiled it.  Set it before
+                             calling sph_default_opts; sph_default_opts and every call
+                             that takes options refuse any other value with
+                             SPH_ERR_ARG, so a caller built against another layout of
+                             this struct cannot make the library read or write past
+                             the caller's copy */
     int fluid;            /* 1: the file has a fluid section (the reference's --fluid) */
     int device;           /* CUDA device ordinal; -1 keeps the current device */
     int verbose;          /* 1: progress on stdout like DEM::startTime */
@@ -65,7 +71,25 @@ typedef struct sph_opts {
     int step_kernel;      /* 0 automatic (the fused persistent step where it applies),
                              1 per-stage kernels, 2 fused persistent step (error where
                              it does not apply: bonds, fluid, wmode 3) */
+    int darcy_exact_stop; /* 1: the Darcy Jacobi loop tests the residual at every
+                             iteration and stops at the first that meets the
+                             tolerance; 0 (default): the reference's test at
+                             iterations 0, 10, 20, ... (src/device.cu:2340-2366) */
+    int inject_timeout;   /* test knob, 0 in normal use: a mask of SPH_INJECT_*.  The
+                             bounded device waits of the selected cooperative kernels
+                             then wait for a value that nothing writes and give up
+                             after about a thousand polls, so the step returns
+                             SPH_ERR_TIMEOUT; this exercises the timeout path without
+                             a GPU fault.  An engine that timed out is closed. */
 } sph_opts;
+
+/* Kernels whose waits sph_opts.inject_timeout makes time out. */
+enum {
+    SPH_INJECT_RESORT = 1,     /* the grid barrier of the cooperative cell re-sort */
+    SPH_INJECT_PERSISTENT = 2, /* the group barrier of the fused persistent step */
+    SPH_INJECT_DARCY = 4,      /* the neighbour waits of the Darcy Jacobi kernel */
+    SPH_INJECT_NS = 8,         /* the barrier and waits of the Navier-Stokes Jacobi kernel */
+};
 
 /* Fields for sph_get/sph_set.  Vector fields use the reference's Float4
  * layout (4 doubles per particle, src/datatypes.h:16-33) in ORIGINAL
@@ -141,8 +165,10 @@ typedef struct sph_info {
     int32_t tuned;        /* 1 once the autotuner has run */
 } sph_info;
 
-/* Fills *opts with the defaults (faithful FP64, TY3, 32 slots, device -1). */
-void sph_default_opts(sph_opts *opts);
+/* Fills *opts with the defaults (faithful FP64, TY3, 32 slots, device -1).
+ * The caller sets opts->struct_size = sizeof(sph_opts) first; any other
+ * value returns SPH_ERR_ARG and writes nothing. */
+int sph_default_opts(sph_opts *opts);
 
 /* Reads and validates a .bin file without touching the device: the
  * reference's `sphere --dry` (src/sphere.cpp:46-51: read, checkValues,
@@ -271,10 +297,14 @@ void sph_close(sph_engine *e);
  * (cudaGetSymbolAddress); later calls reuse it.  Every call shares that one
  * array, so calls whose work overlaps on the GPU (another stream, another
  * thread) race: serialise them.  `stream` is a cudaStream_t (NULL = legacy
- * default stream); the call waits for its own work.  Returns SPH_OK,
- * SPH_ERR_ARG, SPH_ERR_OUTSIDE (a position outside the grid) or
- * SPH_ERR_CUDA; sph_noalloc_error() describes the last failure. */
+ * default stream); the call waits for its own work.  A cell holding more
+ * than SPH_NOALLOC_MAX_PER_CELL particles (a grid far coarser than a contact
+ * search uses) is rejected with SPH_ERR_ARG rather than ordered by a slow
+ * loop.  Returns SPH_OK, SPH_ERR_ARG, SPH_ERR_OUTSIDE (a position outside
+ * the grid) or SPH_ERR_CUDA; sph_noalloc_error() describes the calling
+ * thread's last failure (the message is thread-local). */
 #define SPH_NOALLOC_MAX_CELLS (1u << 20)
+#define SPH_NOALLOC_MAX_PER_CELL 512u
 int sph_sort_cells_noalloc(const double *x4, uint32_t np, const double origo[3],
                            const double L[3], const uint32_t num[3], uint32_t *cellid,
                            uint32_t *index, uint32_t *cell_start, uint32_t *cell_end,

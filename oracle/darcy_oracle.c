@@ -27,6 +27,8 @@ struct orc_darcy {
     double p_top_orig;
     unsigned wall0_iz;
     int64_t nijac_last, nijac_total;
+    int exact_stop; /* test the residual every iteration (the engine's option);
+                       0: at iterations 0, 10, 20, ... as device.cu:2340-2366 */
 };
 
 /* d_idx, src/darcy.cuh:128-137 (unsigned arithmetic like the reference) */
@@ -471,18 +473,22 @@ static double dp_of(const orc_state *s, const struct orc_darcy *D, const double 
     return dp;
 }
 
+/* maxNormResDarcy, darcy.cpp:266-292 (a maximum: the order of the scan
+ * does not change it) */
 static double max_norm(orc_state *s, struct orc_darcy *D, int *nan)
 {
     double m = -1.0e9;
-    *nan = 0;
+    int bad = 0;
+#pragma omp parallel for reduction(max : m) reduction(| : bad) schedule(static)
     for (int z = 0; z < D->nz; ++z)
         for (int y = 0; y < D->ny; ++y)
             for (int x = 0; x < D->nx; ++x) {
                 double v = fabs(D->norm[didx(D, x, y, z)]);
-                if (v != v) { *nan = 1; return v; }
-                if (v > m) m = v;
+                if (v != v) bad = 1;
+                else if (v > m) m = v;
             }
     (void)s;
+    *nan = bad;
     return m;
 }
 
@@ -535,6 +541,8 @@ int orc_darcy_step(orc_state *s)
             for (int z = 0; z < nz; ++z)
                 for (int y = 0; y < ny; ++y)
                     for (int x = 0; x < nx; ++x) D->dp_expl[didx(D, x, y, z)] = dp_of(s, D, D->p, x, y, z);
+        /* every cell reads the previous iterate only: the cells are independent */
+#pragma omp parallel for schedule(static)
         for (int z = 0; z < nz; ++z)
             for (int y = 0; y < ny; ++y)
                 for (int x = 0; x < nx; ++x) {
@@ -556,11 +564,12 @@ int orc_darcy_step(orc_state *s)
                         D->p[didx(D, x, y, (int)zz)] = D->p[didx(D, x, y, (int)zz - 2)];
         }
         if (flux) ghost_flux(s, D);
+#pragma omp parallel for schedule(static)
         for (int z = 0; z < nz; ++z)
             for (int y = 0; y < ny; ++y)
                 for (int x = 0; x < nx; ++x) D->p[didx(D, x, y, z)] = D->p_new[didx(D, x, y, z)];
         done = nijac;
-        if (nijac % 10 == 0) {
+        if (D->exact_stop || nijac % 10 == 0) {
             int nan;
             double m = max_norm(s, D, &nan);
             if (nan) {
@@ -630,4 +639,16 @@ int64_t orc_darcy_get(orc_state *s, const char *name, void *dst, size_t bytes)
                 for (int c = 0; c < comps; ++c)
                     o[(((size_t)z * D->ny + y) * D->nx + x) * comps + c] = f[(size_t)didx(D, x, y, z) * comps + c];
     return 0;
+}
+
+/* Option flags of the Darcy block: "darcy_exact_stop" (one int). */
+int orc_darcy_set(orc_state *s, const char *name, const void *src, size_t bytes)
+{
+    struct orc_darcy *D = s->darcy;
+    if (!D) return -1;
+    if (!strcmp(name, "darcy_exact_stop") && bytes == sizeof(int)) {
+        memcpy(&D->exact_stop, src, sizeof(int));
+        return 0;
+    }
+    return -1;
 }

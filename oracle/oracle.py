@@ -15,7 +15,17 @@ import numpy
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libsphere_ref.so")
-REF_SRC_DEFAULT = "/root/reference/src"
+# The reference tree (read-only), where it is mounted: the host build of its
+# kernels and the tests that read its files use it; machines without it skip
+# them.  $SPHERE_REF_ROOT overrides the location.
+REF_ROOT = os.environ.get("SPHERE_REF_ROOT", "/root/reference")
+
+
+def ref_path(*parts):
+    """Path of a file or directory of the reference tree, or None where the
+    tree (or that entry) is absent."""
+    p = os.path.join(REF_ROOT, *parts)
+    return p if os.path.exists(p) else None
 
 _FIELD4 = {"x", "vel", "angvel", "angpos", "force", "torque", "acc", "angacc",
            "xyzsum", "walls_nx", "walls_mvfd", "bonds_delta", "bonds_omega"}
@@ -26,8 +36,8 @@ _U32 = {"cellid", "index", "cellstart", "cellend", "contacts", "bonds"}
 def build(ref: bool = True) -> None:
     """Compile liboracle.so and, when the reference sources exist, _ref."""
     subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
-    ref_dir = os.environ.get("REF_DIR", REF_SRC_DEFAULT)
-    if ref and os.path.isdir(ref_dir):
+    ref_dir = os.environ.get("REF_DIR") or ref_path("src")
+    if ref and ref_dir and os.path.isdir(ref_dir):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_DIR={ref_dir}"])
 
 

@@ -87,5 +87,6 @@ int orc_darcy_load(struct orc_state *s, const unsigned char **cur,
 int orc_darcy_write(struct orc_state *s, void *fh);
 void orc_darcy_free(struct orc_state *s);
 int64_t orc_darcy_get(struct orc_state *s, const char *name, void *dst, size_t bytes);
+int orc_darcy_set(struct orc_state *s, const char *name, const void *src, size_t bytes);
 
 #endif

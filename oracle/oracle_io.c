@@ -222,6 +222,7 @@ int64_t orc_get(orc_state *s, const char *name, void *dst, size_t bytes)
 
 int orc_set(orc_state *s, const char *name, const void *src, size_t bytes)
 {
+    if (!strncmp(name, "darcy_exact_stop", 16)) return orc_darcy_set(s, name, src, bytes);
     void *ptr;
     int64_t need = locate(s, name, &ptr);
     if (need < 0 || bytes != (size_t)need) return -1;

@@ -23,6 +23,7 @@ Workloads (the sizes of the published benchmark configurations):
 from __future__ import annotations
 
 import math
+import os
 
 import numpy
 
@@ -324,13 +325,73 @@ def settle_packing(n: int = 100000, seed: int = 1, r_min: float = 0.008,
     return state
 
 
-def settled_packing(n: int = 100000, seed: int = 1, cache_dir=None, log=None) -> BinData:
-    """The settled packing of the benchmark workloads (cached as a .bin file
-    under cache_dir, default $SPHB_CACHE or /tmp/sphere_b200_cache)."""
-    import os
+DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+
+
+def _fixture_path(n: int, seed: int) -> str:
+    return os.path.join(DATA_DIR, f"settled_packing_n{n}_seed{seed}.npz")
+
+
+def _byte_planes(a: numpy.ndarray) -> numpy.ndarray:
+    """float64 array -> its 8 byte planes (the sign/exponent planes of
+    positions in a box compress far better apart)."""
+    b = numpy.ascontiguousarray(a, dtype="<f8").view(numpy.uint8).reshape(-1, 8)
+    return numpy.ascontiguousarray(b.T)
+
+
+def _from_planes(p: numpy.ndarray, shape) -> numpy.ndarray:
+    return numpy.ascontiguousarray(p.T).view("<f8").reshape(shape)
+
+
+def pack_fixture(state: BinData, seed: int) -> str:
+    """Stores a settled packing (positions, radii and grid of the state
+    settle_packing returns; every other field of that state is zero or a
+    default) as the packaged fixture of (np, seed)."""
+    os.makedirs(DATA_DIR, exist_ok=True)
+    path = _fixture_path(state.np, seed)
+    numpy.savez_compressed(path, x_planes=_byte_planes(state.x),
+                           radius_planes=_byte_planes(state.radius),
+                           L=state.L, num=state.num, origo=state.origo,
+                           recipe=numpy.array(f"configs.settle_packing(n={state.np}, seed={seed})"))
+    return path
+
+
+def _load_fixture(n: int, seed: int):
+    path = _fixture_path(n, seed)
+    if not os.path.exists(path):
+        return None
+    z = numpy.load(path)
+    d = BinData()
+    _particles(d, n)
+    d.x = _from_planes(z["x_planes"], (n, 3))
+    d.radius = _from_planes(z["radius_planes"], (n,))
+    default_params(d, mu_s=0.5, mu_d=0.5, k_n=1.16e7, k_t=1.16e7)
+    d.g = numpy.array([0.0, 0.0, -9.81])
+    d.origo = numpy.array(z["origo"], dtype=numpy.float64)
+    d.L = numpy.array(z["L"], dtype=numpy.float64)
+    d.num = numpy.array(z["num"], dtype=numpy.uint32)
+    d.periodic = 1
+    d.time_dt = time_step(d)
+    d.time_total = 1e9
+    d.time_file_dt = 1e9
+    return d
+
+
+def settled_packing(n: int = 100000, seed: int = 1, cache_dir=None, log=None,
+                    packaged: bool = True) -> BinData:
+    """The settled packing of the benchmark workloads: the packaged fixture
+    where one exists for (n, seed) (no device is touched), else a .bin cached
+    under cache_dir (default $SPHB_CACHE, or a folder in the system's
+    temporary directory), else settled on the GPU engine and cached."""
+    import tempfile
     from .binfile import read_bin, write_bin
 
-    cache_dir = cache_dir or os.environ.get("SPHB_CACHE", "/tmp/sphere_b200_cache")
+    if packaged:
+        d = _load_fixture(n, seed)
+        if d is not None:
+            return d
+    cache_dir = cache_dir or os.environ.get("SPHB_CACHE") or os.path.join(
+        tempfile.gettempdir(), "sphere_b200_cache")
     os.makedirs(cache_dir, exist_ok=True)
     path = os.path.join(cache_dir, f"packing4_n{n}_seed{seed}.bin")
     if os.path.exists(path):

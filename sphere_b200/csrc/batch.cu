@@ -93,6 +93,7 @@ struct BatchEngine {
         set_sync_args(A, sync);
         A.group_size = g;
         A.nsteps = (unsigned)n;
+        A.inject = (boxes[0]->inject & sphb::kInjectPersistent) ? 1u : 0u;
         return persistent_launch(prec, model, sh, A, gr,
                                  persistent_smem(kPersistShapes[sh].threads, ncmax), stream);
     }
@@ -238,9 +239,17 @@ int batch_open(int nbox, const char *const *paths, const void *const *bufs, cons
     if (!out || nbox <= 0) return SPH_ERR_ARG;
     *out = nullptr;
     auto B = std::make_unique<BatchEngine>();
+    if (opts && opts->struct_size != sizeof(sph_opts)) {
+        g_batch_open_error = "sph_opts.struct_size does not match this library's sph_opts";
+        return SPH_ERR_ARG;
+    }
     sph_opts o;
-    if (opts) o = *opts;
-    else sph_default_opts(&o);
+    if (opts) {
+        o = *opts;
+    } else {
+        o.struct_size = sizeof(sph_opts);
+        sph_default_opts(&o);
+    }
     o.step_kernel = 2;   // every box must run on the fused step
     o.fluid = 0;
     for (int i = 0; i < nbox; ++i) {

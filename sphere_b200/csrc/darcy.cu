@@ -32,6 +32,7 @@ struct DarcyParams {
     double bc_bot_flux, bc_top_flux;
     int bc_xn, bc_xp, bc_yn, bc_yp, bc_bot, bc_top;
     unsigned maxiter, ndem;
+    unsigned inject;               // 1: the Jacobi waits never succeed (a test knob)
 };
 
 struct DarcyCtl {
@@ -541,15 +542,18 @@ __device__ __forceinline__ double dp_fast(const DarcyParams &D, const JacobiCoef
 
 // Bounded wait of thread 0 until *p >= target; false (and DERR_TIMEOUT in
 // the engine's error flag) after ~2^22 polls, or as soon as another block
-// has flagged an error.
-__device__ __forceinline__ bool jacobi_wait_ge(const unsigned *p, unsigned target, DarcyCtl *ctl)
+// has flagged an error.  With `inject` the wait never succeeds and gives up
+// after kInjectPolls polls.
+__device__ __forceinline__ bool jacobi_wait_ge(const unsigned *p, unsigned target, DarcyCtl *ctl,
+                                               unsigned inject)
 {
     unsigned spins = 0, nap = 16;
+    const unsigned limit = inject ? kInjectPolls : (1u << 22);
     for (;;) {
         unsigned v;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-        if (v >= target) return true;
-        if (++spins > (1u << 22)) {
+        if (v >= target && !inject) return true;
+        if (++spins > limit) {
             atomicCAS(&ctl->err, 0, DERR_TIMEOUT);
             return false;
         }
@@ -608,7 +612,7 @@ __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, Ja
     auto decide = [&](unsigned c) {
         const unsigned k = dec_count;
         // acquire: every block's residual (ordered before its release-add)
-        if (!jacobi_wait_ge(&js->arrive[k % kJacobiChecks][0], G, ctl)) {
+        if (!jacobi_wait_ge(&js->arrive[k % kJacobiChecks][0], G, ctl, D.inject)) {
             s_state = 2;
             return;
         }
@@ -650,7 +654,7 @@ __global__ void __launch_bounds__(256) k_jacobi(DarcyParams D, DarcyFields F, Ja
                 // the lanes of warp 0 watch the neighbours in parallel
                 bool ok = true;
                 for (unsigned q = nb_lo + threadIdx.x; q <= nb_hi; q += 32)
-                    if (q != b && !jacobi_wait_ge(&js->done[q][0], it, ctl)) ok = false;
+                    if (q != b && !jacobi_wait_ge(&js->done[q][0], it, ctl, D.inject)) ok = false;
                 if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0) s_state = 2;
             }
         }
@@ -844,6 +848,7 @@ int Engine::darcy_init()
     D.bc_xn = hs.bc_xn; D.bc_xp = hs.bc_xp; D.bc_yn = hs.bc_yn; D.bc_yp = hs.bc_yp;
     D.bc_bot = hs.bc_bot; D.bc_top = hs.bc_top;
     D.maxiter = hs.maxiter; D.ndem = hs.ndem;
+    D.inject = (inject & kInjectDarcy) ? 1u : 0u;
     const size_t nx = D.nx, ny = D.ny, nz = D.nz;
     const size_t ng = (nx + 2) * (ny + 2) * (nz + 2);
     Dd.ng = ng;

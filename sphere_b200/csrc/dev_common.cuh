@@ -24,6 +24,13 @@ enum DevErr : int {
     DERR_NAN = 5,       // Darcy residual not finite
 };
 
+// Fault injection for tests (sph_opts.inject_timeout, values equal to
+// SPH_INJECT_*): the bounded waits of the selected kernels wait for a value
+// nothing writes and give up after kInjectPolls polls, so the error path of a
+// timed-out wait runs without a real hang.
+constexpr uint32_t kInjectResort = 1, kInjectPersistent = 2, kInjectDarcy = 4, kInjectNS = 8;
+constexpr unsigned kInjectPolls = 1u << 10;
+
 // Per-run constants, passed to every kernel by value.
 struct DevParams {
     uint32_t np, nc, nw, nb0;
@@ -43,6 +50,7 @@ struct DevParams {
     double lambda_bar, sigma_b, tau_b;
     double skin;                   // neighbour-list skin [m]
     uint32_t nlmax;                // neighbour-list entries per particle
+    uint32_t inject;               // kInject* mask (a test knob; 0 in normal use)
 };
 
 // Loop state that lives on the device so captured graphs can replay steps.

@@ -119,6 +119,7 @@ void Engine::build_params()
     for (uint32_t i = 0; i < h.np; ++i) rmin = std::min(rmin, h.x[i].w);
     p.skin = h.np ? 0.1 * rmin : 0.0;
     p.nlmax = nlmax;
+    p.inject = inject;
 }
 
 int Engine::allocate_and_upload()
@@ -778,6 +779,10 @@ int Engine::run()
 
 }  // namespace sphb
 
+static_assert(sphb::kInjectResort == SPH_INJECT_RESORT && sphb::kInjectPersistent == SPH_INJECT_PERSISTENT &&
+                  sphb::kInjectDarcy == SPH_INJECT_DARCY && sphb::kInjectNS == SPH_INJECT_NS,
+              "fault-injection bits of the device code and the C ABI");
+
 using sphb::Engine;
 
 struct sph_engine {
@@ -786,22 +791,30 @@ struct sph_engine {
 
 extern "C" {
 
-void sph_default_opts(sph_opts *o)
+int sph_default_opts(sph_opts *o)
 {
-    if (!o) return;
+    // the caller's struct_size is read before anything is written: a caller
+    // compiled against another layout gets an error, not an overwrite
+    if (!o || o->struct_size != sizeof(sph_opts)) return SPH_ERR_ARG;
     std::memset(o, 0, sizeof *o);
+    o->struct_size = sizeof(sph_opts);
     o->device = -1;
     o->precision = SPH_PREC_FAITHFUL;
     o->integrator = 3;
     o->contact_capacity = 32;
     o->graph_steps = 0;
+    return SPH_OK;
 }
 
 static int open_common(std::unique_ptr<Engine> &eng, const sph_opts *opts)
 {
     sph_opts o;
-    if (opts) o = *opts;
-    else sph_default_opts(&o);
+    if (opts) {
+        o = *opts;
+    } else {
+        o.struct_size = sizeof(sph_opts);
+        sph_default_opts(&o);
+    }
     Engine &e = *eng;
     e.precision = o.precision;
     e.integrator = o.integrator == 2 ? 2 : 3;
@@ -814,6 +827,8 @@ static int open_common(std::unique_ptr<Engine> &eng, const sph_opts *opts)
     e.graph_steps = o.graph_steps > 0 ? o.graph_steps : 64;
     e.warm_start = o.warm_start;
     e.step_kernel = o.step_kernel;
+    e.darcy_exact_stop = o.darcy_exact_stop ? 1 : 0;
+    e.inject = (uint32_t)o.inject_timeout;
     e.outdir = o.output_dir ? o.output_dir : "output";
     if (e.precision != SPH_PREC_FAITHFUL && e.precision != SPH_PREC_FP64 &&
         e.precision != SPH_PREC_MIXED)
@@ -862,6 +877,10 @@ int sph_open(const char *bin_path, const sph_opts *opts, sph_engine **out)
 {
     if (!bin_path || !out) return SPH_ERR_ARG;
     *out = nullptr;
+    if (opts && opts->struct_size != sizeof(sph_opts)) {
+        sphb::g_open_error = "sph_opts.struct_size does not match this library's sph_opts";
+        return SPH_ERR_ARG;
+    }
     auto eng = std::make_unique<Engine>();
     int fluid = opts ? opts->fluid : 0;
     int rc = sphb::read_bin_file(bin_path, fluid, eng->hs, eng->err);
@@ -882,6 +901,10 @@ int sph_open_buffer(const void *bytes, size_t nbytes, const sph_opts *opts, cons
 {
     if (!bytes || !out) return SPH_ERR_ARG;
     *out = nullptr;
+    if (opts && opts->struct_size != sizeof(sph_opts)) {
+        sphb::g_open_error = "sph_opts.struct_size does not match this library's sph_opts";
+        return SPH_ERR_ARG;
+    }
     auto eng = std::make_unique<Engine>();
     int fluid = opts ? opts->fluid : 0;
     int rc = sphb::parse_bin((const uint8_t *)bytes, nbytes, fluid, eng->hs, eng->err);
@@ -908,6 +931,10 @@ namespace sphb {
 int open_engine(const char *path, const void *bytes, size_t nbytes, const sph_opts *opts,
                 const char *sid, std::unique_ptr<Engine> &out, std::string &err)
 {
+    if (opts && opts->struct_size != sizeof(sph_opts)) {
+        err = "sph_opts.struct_size does not match this library's sph_opts";
+        return SPH_ERR_ARG;
+    }
     auto eng = std::make_unique<Engine>();
     int fluid = opts ? opts->fluid : 0;
     int rc = path ? read_bin_file(path, fluid, eng->hs, eng->err)

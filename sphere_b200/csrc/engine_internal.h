@@ -37,6 +37,7 @@ public:
     int warm_start = 0;
     int warm_start_train = 2000;  // solves the warm-start network trains on
     int step_kernel = 0;          // 0 automatic, 1 per-stage kernels, 2 persistent
+    uint32_t inject = 0;          // SPH_INJECT_* mask (a test knob; 0 in normal use)
     std::string outdir = "output";
     std::string sid = "unnamed";
 

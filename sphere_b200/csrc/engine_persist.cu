@@ -139,6 +139,7 @@ cudaError_t Engine::persist_launch(uint64_t n, int shape, unsigned grid)
     set_sync_args(A, D.sync);
     A.group_size = grid;
     A.nsteps = (unsigned)n;
+    A.inject = (inject & kInjectPersistent) ? 1u : 0u;
     return persistent_launch(precision, (int)hs.contactmodel, shape, A, grid,
                              persistent_smem(threads, capacity), stream);
 }

@@ -42,6 +42,7 @@ struct NSParams {
     double g[3];
     int bc_bot, bc_top;
     unsigned maxiter, ndem, np;
+    unsigned inject;                // 1: the Jacobi waits never succeed (a test knob)
 };
 
 struct NSCtl {
@@ -581,7 +582,9 @@ __global__ void k_forcing_const(NSParams N, const double *phi_a, const double *d
 
 // Bounded grid barrier of the cooperative Jacobi kernel: after ~2^24 polls
 // it records DERR_TIMEOUT and returns false instead of spinning forever.
-__device__ bool ns_barrier(NSCtl *ctl, unsigned nblocks)
+// With `inject` no block releases it and every block gives up after
+// kInjectPolls polls.
+__device__ bool ns_barrier(NSCtl *ctl, unsigned nblocks, unsigned inject)
 {
     __syncthreads();
     __shared__ int ok;
@@ -591,14 +594,15 @@ __device__ bool ns_barrier(NSCtl *ctl, unsigned nblocks)
         __threadfence();
         const unsigned arrived = atomicAdd(&ctl->barrier_count, 1u);
         ok = 1;
-        if (arrived == nblocks - 1) {
+        if (arrived == nblocks - 1 && !inject) {
             ctl->barrier_count = 0;
             __threadfence();
             atomicAdd(&ctl->barrier_gen, 1u);
         } else {
             unsigned spins = 0;
-            while (*gen == g) {
-                if (++spins > (1u << 24)) {
+            const unsigned limit = inject ? kInjectPolls : (1u << 24);
+            while (inject || *gen == g) {
+                if (++spins > limit) {
                     atomicCAS(&ctl->err, 0, (int)DERR_TIMEOUT);
                     ok = 0;
                     break;
@@ -643,14 +647,16 @@ __device__ __forceinline__ double ldg(const double *p) { return __ldcg(p); }
 // Waits (thread-wise, bounded) until *p >= target with acquire semantics;
 // records DERR_TIMEOUT after ~2^22 polls or stops when another block has
 // flagged an error.
-__device__ __forceinline__ bool ns_wait_ge(const unsigned *p, unsigned target, NSCtl *ctl)
+__device__ __forceinline__ bool ns_wait_ge(const unsigned *p, unsigned target, NSCtl *ctl,
+                                           unsigned inject)
 {
     unsigned spins = 0, nap = 16;
+    const unsigned limit = inject ? kInjectPolls : (1u << 22);
     for (;;) {
         unsigned v;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-        if (v >= target) return true;
-        if (++spins > (1u << 22)) {
+        if (v >= target && !inject) return true;
+        if (++spins > limit) {
             atomicCAS(&ctl->err, 0, (int)DERR_TIMEOUT);
             return false;
         }
@@ -680,7 +686,7 @@ __global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ct
         // P[2] carries the loop's incoming ghost nodes (read by the first
         // forcing); P[0] gets the fresh ghosts of E_0
         for (unsigned q = tid; q < ng; q += stride) J.b2[q] = J.eps[q];
-        ok = ns_barrier(ctl, gridDim.x);
+        ok = ns_barrier(ctl, gridDim.x, N.inject);
         if (ok) {
             for (unsigned i = tid; i < nc; i += stride) {
                 int x, y, z;
@@ -688,7 +694,7 @@ __global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ct
                 const double val = J.eps[cix(N, x, y, z)];
                 ghost_cell<1>(N, J.eps, x, y, z, &val);
             }
-            ok = ns_barrier(ctl, gridDim.x);
+            ok = ns_barrier(ctl, gridDim.x, N.inject);
         }
     }
     // this block's cells and the blocks whose cells its iteration reads
@@ -705,7 +711,7 @@ __global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ct
     // the stop rule of check iteration c (thread 0): every block's maximum
     auto decide = [&](unsigned c) {
         const unsigned k = c / 10u;
-        if (!ns_wait_ge(&S->arrive[k % kNSChecks][0], G, ctl)) {
+        if (!ns_wait_ge(&S->arrive[k % kNSChecks][0], G, ctl, N.inject)) {
             s_state = 2;
             return;
         }
@@ -731,7 +737,7 @@ __global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ct
                 // the lanes of warp 0 watch the neighbours in parallel
                 bool okw = true;
                 for (unsigned q = nb_lo + threadIdx.x; q <= nb_hi; q += 32)
-                    if (q != b && !ns_wait_ge(&S->done[q][0], nijac, ctl)) okw = false;
+                    if (q != b && !ns_wait_ge(&S->done[q][0], nijac, ctl, N.inject)) okw = false;
                 if (!__all_sync(0xffffffffu, okw) && threadIdx.x == 0) s_state = 2;
             }
         }
@@ -813,7 +819,7 @@ __global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ct
     if (s_state == 2) ok = false;
     conv = s_state == 1;
     // every block's cells before the final copy
-    if (ok && last >= 0) ok = ns_barrier(ctl, gridDim.x);
+    if (ok && last >= 0) ok = ns_barrier(ctl, gridDim.x, N.inject);
     if (ok && last >= 0) {
         const double *fin = P((unsigned)((last + 1) % 3));
         const double *gsrc = conv ? fin : P((unsigned)(last % 3));
@@ -829,7 +835,7 @@ __global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ct
     if (ok && conv && N.gamma > 0.0) {
         // smoothing<Float>, navierstokes.cuh:2619-2677, reading the whole
         // field before writing, then the ghost nodes again
-        ok = ns_barrier(ctl, gridDim.x);
+        ok = ns_barrier(ctl, gridDim.x, N.inject);
         if (ok) {
             for (unsigned i = tid; i < nc; i += stride) {
                 int x, y, z;
@@ -845,7 +851,7 @@ __global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ct
                 const double e_avg = 1.0 / 6.0 * (e_xn + e_xp + e_yn + e_yp + e_zn + e_zp);
                 J.tmp[c] = (1.0 - N.gamma) * e + N.gamma * e_avg;
             }
-            ok = ns_barrier(ctl, gridDim.x);
+            ok = ns_barrier(ctl, gridDim.x, N.inject);
         }
         if (ok) {
             for (unsigned i = tid; i < nc; i += stride) {
@@ -855,7 +861,7 @@ __global__ void __launch_bounds__(NT) k_jacobi(NSParams N, NSJacobi J, NSCtl *ct
                 const unsigned c = cix(N, x, y, z);
                 J.eps[c] = ldg(&J.tmp[c]);
             }
-            ok = ns_barrier(ctl, gridDim.x);
+            ok = ns_barrier(ctl, gridDim.x, N.inject);
         }
         if (ok) {
             for (unsigned i = tid; i < nc; i += stride) {
@@ -946,6 +952,7 @@ int Engine::ns_init()
     for (int k = 0; k < 3; ++k) N.g[k] = hs.g[k];
     N.bc_bot = hs.bc_bot; N.bc_top = hs.bc_top;
     N.maxiter = hs.maxiter; N.ndem = hs.ndem; N.np = hs.np;
+    N.inject = (inject & kInjectNS) ? 1u : 0u;
     const size_t nx = N.nx, ny = N.ny, nz = N.nz;
     D.ng = (nx + 2) * (ny + 2) * (nz + 2);
     D.ngf = (nx + 3) * (ny + 3) * (nz + 3);

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/sphere_b200.h"
+#include "cell_order.cuh"
 
 namespace sphb {
 namespace {
@@ -26,6 +27,7 @@ constexpr size_t kOffFill = kMaxCells;
 constexpr size_t kOffTiles = 2 * (size_t)kMaxCells;
 constexpr size_t kOffErr = kOffTiles + kMaxTiles;
 constexpr size_t kWords = kOffErr + 64;
+static_assert(kCellRankMax == SPH_NOALLOC_MAX_PER_CELL, "per-cell limit of the header");
 
 // Scratch shared by every call of sph_sort_cells_noalloc on a device.  It is
 // resident on every GPU that loads this library (about 8.4 MB) until exit.
@@ -142,32 +144,33 @@ __global__ void k_na_scatter(const double *x4, uint32_t np, Grid g, uint32_t *sc
     index[pos] = i;
 }
 
-// Orders each cell's entries by original index (the stable sort order) and
-// writes the sorted cell keys.
+// Orders each cell's entries by original index (the stable sort order),
+// one warp per cell with the engine's register ranks, and writes the sorted
+// cell keys.  A cell of more than kCellRankMax entries is not ordered: it
+// raises error 2 (a grid far coarser than the contact search uses), so no
+// call runs a quadratic loop over a crowded cell.
 __global__ void k_na_cells(uint32_t *scr, uint32_t ncells, const uint32_t *cell_end,
                            uint32_t *index, uint32_t *cellid)
 {
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (c >= ncells || scr[kOffErr]) return;
-    uint32_t n = scr[kOffCount + c];
+    const uint32_t n = scr[kOffCount + c];
     if (n == 0) return;
-    uint32_t b = cell_end[c] - n;
-    for (uint32_t i = b + 1; i < b + n; ++i) {
-        uint32_t v = index[i];
-        uint32_t j = i;
-        while (j > b && index[j - 1] > v) {
-            index[j] = index[j - 1];
-            --j;
-        }
-        index[j] = v;
+    const uint32_t b = cell_end[c] - n;
+    if (n > kCellRankMax) {
+        if (lane == 0 && atomicCAS(&scr[kOffErr], 0u, 2u) == 0u) scr[kOffErr + 1] = c;
+        return;
     }
-    for (uint32_t i = b; i < b + n; ++i) cellid[i] = c;
+    if (n > 1) warp_rank_order(index, b, n, lane);
+    for (uint32_t i = b + lane; i < b + n; i += 32u) cellid[i] = c;
 }
 
 // Device address of g_noalloc_scratch, looked up once per device.
 std::mutex g_mu;
 uint32_t *g_scratch_ptr[64] = {};
-char g_err[256];
+// message of the calling thread's last failure
+thread_local char g_err[256];
 
 int scratch_for_current_device(uint32_t **out)
 {
@@ -231,7 +234,8 @@ extern "C" int sph_sort_cells_noalloc(const double *x4, uint32_t np, const doubl
     k_na_scan_tiles<<<1, kTile, 0, st>>>(scr, ntiles);
     k_na_apply<<<ntiles, kTile, 0, st>>>(scr, nc, cell_start, cell_end);
     if (np) k_na_scatter<<<(np + 255) / 256, 256, 0, st>>>(x4, np, g, scr, cell_end, index);
-    k_na_cells<<<(nc + 255) / 256, 256, 0, st>>>(scr, nc, cell_end, index, cellid);
+    k_na_cells<<<(unsigned)(((uint64_t)nc * 32 + 255) / 256), 256, 0, st>>>(scr, nc, cell_end, index,
+                                                                               cellid);
     cudaError_t e = cudaGetLastError();
     uint32_t flag[2] = {0, 0};
     if (e == cudaSuccess)
@@ -240,6 +244,12 @@ extern "C" int sph_sort_cells_noalloc(const double *x4, uint32_t np, const doubl
     if (e != cudaSuccess) {
         std::snprintf(g_err, sizeof g_err, "CUDA error: %s", cudaGetErrorString(e));
         return SPH_ERR_CUDA;
+    }
+    if (flag[0] == 2) {
+        std::snprintf(g_err, sizeof g_err,
+                      "cell %u holds more than %u particles: the grid is too coarse", flag[1],
+                      kCellRankMax);
+        return SPH_ERR_ARG;
     }
     if (flag[0]) {
         std::snprintf(g_err, sizeof g_err, "particle %u is outside the grid or not finite", flag[1]);

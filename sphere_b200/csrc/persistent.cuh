@@ -90,19 +90,22 @@ struct BatchArgs {
     unsigned nsteps;
     int *abort;                // set when a barrier gave up; every group stops
     int *any_err;              // set when some box raised an error
+    unsigned inject;           // 1: the group barriers never release (a test knob)
 };
 
 // Barrier over the blocks of one group, bounded: after ~2^24 polls it sets
 // *abort and returns false, and every waiting block returns false as soon
 // as it sees *abort.  Groups of more than 64 blocks (only ever group 0: a
 // single box stepped by the whole grid) arrive in two levels so no counter
-// takes more than ~64 serialised atomics.
+// takes more than ~64 serialised atomics.  With `inject` no block releases
+// the barrier and every block gives up after kInjectPolls polls.
 __device__ __forceinline__ bool group_barrier(GroupSync *g, GroupTree *tree, unsigned size,
-                                              unsigned rank, int *abort)
+                                              unsigned rank, int *abort, bool inject)
 {
     if (size == 1) {
         __syncthreads();
-        return true;
+        if (inject && threadIdx.x == 0) atomicExch(abort, 1);
+        return !inject;
     }
     __shared__ int ok;
     __syncthreads();
@@ -124,14 +127,15 @@ __device__ __forceinline__ bool group_barrier(GroupSync *g, GroupTree *tree, uns
             last = atomicAdd(&g->count, 1u) == size - 1;
         }
         ok = 1;
-        if (last) {
+        if (last && !inject) {
             g->count = 0;
             __threadfence();
             atomicAdd(&g->gen, 1u);
         } else {
             unsigned spins = 0, nap = 32;
-            while (*gen == cur) {
-                if (++spins > (1u << 24)) {
+            const unsigned limit = inject ? kInjectPolls : (1u << 24);
+            while (inject || *gen == cur) {
+                if (++spins > limit) {
                     atomicExch(abort, 1);
                     ok = 0;
                     break;
@@ -175,7 +179,7 @@ __global__ void __launch_bounds__(NT, MINB) k_persistent(BatchArgs A)
     GroupSync *G = &A.groups[gid];
     const unsigned B = blockDim.x, t = threadIdx.x;
     const unsigned gtid = rank * B + t, gstride = gsz * B;
-    auto bar = [&]() { return group_barrier(G, A.tree, gsz, rank, A.abort); };
+    auto bar = [&]() { return group_barrier(G, A.tree, gsz, rank, A.abort, A.inject != 0); };
 
     for (;;) {
         // ---- take the next box ----

@@ -13,6 +13,7 @@
 #pragma once
 
 #include "dem_state.h"
+#include "cell_order.cuh"
 
 namespace sphb {
 
@@ -142,44 +143,17 @@ __device__ bool resort_group(const DevParams &P, const DevState &S, const PermSc
     }
     if (!bar()) return false;
     // 5. order each cell by original index (stable sort order), one warp
-    // per cell: the lanes hold the cell's entries in registers and each
-    // entry's rank is the number of smaller ones (the indices are
-    // distinct), counted over warp shuffles.  Cells of more than 32 x
-    // kRankPer entries fall back to an insertion sort by one lane.
+    // per cell (warp_rank_order).  Cells of more than kCellRankMax entries
+    // fall back to an insertion sort by one lane.
     {
-        constexpr int kRankPer = 16;
         const unsigned lane = threadIdx.x & 31u;
         const unsigned gwarp = gtid >> 5, nwarps = gstride >> 5;
         for (unsigned c = gwarp; c < ncells; c += nwarps) {
             const unsigned n = __ldcg(&S.count[c]);
             if (n < 2) continue;
             const unsigned b = __ldcg(&S.cell_end[c]) - n;
-            if (n <= 32u * kRankPer) {
-                const unsigned kn = (n + 31u) >> 5;   // occupied register rows
-                unsigned v[kRankPer], rk[kRankPer];
-#pragma unroll
-                for (int k = 0; k < kRankPer; ++k) {
-                    const unsigned idx = lane + 32u * k;
-                    v[k] = ((unsigned)k < kn && idx < n) ? __ldcg(&S.vals[b + idx]) : 0xffffffffu;
-                    rk[k] = 0;
-                }
-#pragma unroll
-                for (int k2 = 0; k2 < kRankPer; ++k2) {
-                    if ((unsigned)k2 >= kn) break;
-                    for (unsigned src = 0; src < 32u; ++src) {
-                        const unsigned w = __shfl_sync(0xffffffffu, v[k2], src);
-                        if (32u * k2 + src >= n) break;
-#pragma unroll
-                        for (int k = 0; k < kRankPer; ++k)
-                            if ((unsigned)k < kn) rk[k] += w < v[k] ? 1u : 0u;
-                    }
-                }
-                __syncwarp();
-#pragma unroll
-                for (int k = 0; k < kRankPer; ++k) {
-                    const unsigned idx = lane + 32u * k;
-                    if ((unsigned)k < kn && idx < n) S.vals[b + rk[k]] = v[k];
-                }
+            if (n <= kCellRankMax) {
+                warp_rank_order(S.vals, b, n, lane);
             } else if (lane == 0) {
                 for (unsigned i = b + 1; i < b + n; ++i) {
                     unsigned v = __ldcg(&S.vals[i]);

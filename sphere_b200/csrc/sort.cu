@@ -21,8 +21,9 @@ namespace sphb {
 
 // Grid-wide barrier for a cooperative launch, with a bounded wait: after
 // ~2^24 polls (well over a second) it records DERR_TIMEOUT and returns
-// false instead of spinning forever.
-__device__ bool grid_barrier(DevCtl *ctl, unsigned nblocks)
+// false instead of spinning forever.  With `inject` no block releases it and
+// every block gives up after kInjectPolls polls.
+__device__ bool grid_barrier(DevCtl *ctl, unsigned nblocks, bool inject)
 {
     __syncthreads();
     __shared__ int ok;
@@ -32,14 +33,15 @@ __device__ bool grid_barrier(DevCtl *ctl, unsigned nblocks)
         __threadfence();
         unsigned arrived = atomicAdd(&ctl->barrier_count, 1u);
         ok = 1;
-        if (arrived == nblocks - 1) {
+        if (arrived == nblocks - 1 && !inject) {
             ctl->barrier_count = 0;
             __threadfence();
             atomicAdd(&ctl->barrier_gen, 1u);
         } else {
             unsigned spins = 0;
-            while (*gen == g) {
-                if (++spins > (1u << 24)) {
+            const unsigned limit = inject ? kInjectPolls : (1u << 24);
+            while (inject || *gen == g) {
+                if (++spins > limit) {
                     raise_err(ctl, DERR_TIMEOUT, -1);
                     ok = 0;
                     break;
@@ -67,7 +69,8 @@ __global__ void __launch_bounds__(256, 3) k_resort(DevParams P, DevState S, Perm
     const bool resort = force || ctl->resort;
     const bool nl = with_nl && (resort || ctl->nl_rebuild);
     if (!resort && !nl) return;
-    auto bar = [&]() { return grid_barrier(ctl, gridDim.x); };
+    const bool inject = (P.inject & kInjectResort) != 0;
+    auto bar = [&]() { return grid_barrier(ctl, gridDim.x, inject); };
     if (resort) {
         // the FP32 velocity copies of the mixed mode follow the permutation
         if (!resort_group(P, S, W, gridDim.x, blockIdx.x, bar, true)) return;

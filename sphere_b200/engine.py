@@ -42,11 +42,17 @@ STATUS = {
 
 
 class SphOpts(ctypes.Structure):
-    _fields_ = [("fluid", ctypes.c_int), ("device", ctypes.c_int), ("verbose", ctypes.c_int),
+    _fields_ = [("struct_size", ctypes.c_size_t), ("fluid", ctypes.c_int),
+                ("device", ctypes.c_int), ("verbose", ctypes.c_int),
                 ("precision", ctypes.c_int), ("integrator", ctypes.c_int),
                 ("contact_capacity", ctypes.c_int), ("warm_start", ctypes.c_int),
                 ("graph_steps", ctypes.c_int), ("output_dir", ctypes.c_char_p),
-                ("step_kernel", ctypes.c_int)]
+                ("step_kernel", ctypes.c_int), ("darcy_exact_stop", ctypes.c_int),
+                ("inject_timeout", ctypes.c_int)]
+
+
+# sph_opts.inject_timeout bits (SPH_INJECT_*)
+INJECT = {"resort": 1, "persistent": 2, "darcy": 4, "ns": 8}
 
 
 class SphInfo(ctypes.Structure):
@@ -98,6 +104,7 @@ def lib() -> ctypes.CDLL:
     L = ctypes.CDLL(LIB_PATH)
     P = ctypes.c_void_p
     L.sph_default_opts.argtypes = [ctypes.POINTER(SphOpts)]
+    L.sph_default_opts.restype = ctypes.c_int
     L.sph_open.argtypes = [ctypes.c_char_p, ctypes.POINTER(SphOpts), ctypes.POINTER(P)]
     L.sph_open_buffer.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(SphOpts),
                                   ctypes.c_char_p, ctypes.POINTER(P)]
@@ -163,9 +170,12 @@ STEP_KERNEL = {"auto": 0, "stages": 1, "persistent": 2}
 
 def make_opts(fluid=False, precision="faithful", integrator=3, capacity=32, device=-1,
               graph_steps=0, warm_start=False, verbose=False, output_dir=None,
-              step_kernel="auto") -> SphOpts:
+              step_kernel="auto", darcy_exact_stop=False, inject_timeout=0) -> SphOpts:
     o = SphOpts()
-    lib().sph_default_opts(ctypes.byref(o))
+    o.struct_size = ctypes.sizeof(SphOpts)
+    rc = lib().sph_default_opts(ctypes.byref(o))
+    if rc != 0:
+        raise EngineError(rc, "sph_default_opts refused this build's sph_opts layout")
     o.fluid = int(bool(fluid))
     o.precision = PREC[precision] if isinstance(precision, str) else int(precision)
     o.integrator = int(integrator)
@@ -176,6 +186,10 @@ def make_opts(fluid=False, precision="faithful", integrator=3, capacity=32, devi
     o.verbose = int(bool(verbose))
     o.output_dir = os.fsencode(output_dir) if output_dir else None
     o.step_kernel = STEP_KERNEL[step_kernel] if isinstance(step_kernel, str) else int(step_kernel)
+    o.darcy_exact_stop = int(bool(darcy_exact_stop))
+    if isinstance(inject_timeout, str):
+        inject_timeout = INJECT[inject_timeout]
+    o.inject_timeout = int(inject_timeout)
     return o
 
 
@@ -189,19 +203,22 @@ class Engine:
 
     def __init__(self, source: Union[str, os.PathLike, binfile.BinData], fluid: Optional[bool] = None,
                  precision="faithful", integrator=3, capacity=32, device=-1, graph_steps=0,
-                 warm_start=False, verbose=False, output_dir=None, sid=None, step_kernel="auto"):
+                 warm_start=False, verbose=False, output_dir=None, sid=None, step_kernel="auto",
+                 darcy_exact_stop=False, inject_timeout=0):
         L = lib()
         h = ctypes.c_void_p()
+        extra = dict(darcy_exact_stop=darcy_exact_stop, inject_timeout=inject_timeout)
         if isinstance(source, binfile.BinData):
             fl = source.fluid if fluid is None else fluid
             self._opts = make_opts(fl, precision, integrator, capacity, device, graph_steps,
-                                   warm_start, verbose, output_dir, step_kernel)
+                                   warm_start, verbose, output_dir, step_kernel, **extra)
             buf = binfile.serialize_bin(source)
             rc = L.sph_open_buffer(buf, len(buf), ctypes.byref(self._opts),
                                    (sid or "unnamed").encode(), ctypes.byref(h))
         else:
             self._opts = make_opts(bool(fluid), precision, integrator, capacity, device,
-                                   graph_steps, warm_start, verbose, output_dir, step_kernel)
+                                   graph_steps, warm_start, verbose, output_dir, step_kernel,
+                                   **extra)
             rc = L.sph_open(os.fsencode(source), ctypes.byref(self._opts), ctypes.byref(h))
         if rc < 0 or not h.value:
             raise EngineError(rc, L.sph_open_error().decode())

@@ -6,8 +6,10 @@ import types
 import numpy
 import pytest
 
+import oracle
+
 # the reference's python tree, read-only; present only where it is mounted
-REF_PY = os.environ.get("SPHERE_REF_PY", "/root/reference/python")
+REF_PY = oracle.ref_path("python")
 
 VEC3 = ("angvel", "angpos", "force", "torque", "xyzsum", "acc", "angacc")
 
@@ -70,7 +72,7 @@ def bonded_packing(configs, n=300, seed=21, spacing=0.0195, factor=1.05, max_bon
 def import_reference_sphere():
     """Imports python/sphere.py read-only with stand-ins for what it needs
     but does not use here: matplotlib, and numpy.infty (NumPy 2)."""
-    if not os.path.isdir(REF_PY):
+    if not REF_PY or not os.path.isdir(REF_PY):
         pytest.skip("reference python tree not present")
     for m in ("matplotlib", "matplotlib.pyplot", "matplotlib.collections",
               "matplotlib.colors", "matplotlib.cm", "matplotlib.patches",

@@ -13,7 +13,9 @@ from sphere_b200 import binfile, configs
 
 from helpers import Count as _Count, import_reference_sphere as _import_reference_sphere
 
-REF_OUT = "/root/reference/output"
+import oracle
+
+REF_OUT = oracle.ref_path("output") or ""
 
 
 def test_roundtrip_dry():

@@ -43,6 +43,20 @@ def darcy_case(seed, periodic=1, bottom_no_flow=True, top_wall=True, ndem=1, n=3
     return d
 
 
+def field_errors(eng, orc):
+    """Largest |engine - oracle| of each field over the field's largest
+    magnitude."""
+    errs = {}
+    for a_name, b_name in PAIRS:
+        a = numpy.asarray(eng.get(a_name), dtype=float)
+        b = numpy.asarray(orc.get(b_name), dtype=float)
+        if a_name in ("x", "vel", "force", "darcy_f_p"):
+            a, b = a.reshape(-1, 4)[:, :3], b.reshape(-1, 4)[:, :3]
+        scale = max(float(numpy.abs(b).max()), 1e-300)
+        errs[a_name] = float(numpy.abs(a.ravel() - b.ravel()).max()) / scale
+    return errs
+
+
 def compare(eng, orc):
     bad = {}
     for a_name, b_name in PAIRS:
@@ -170,3 +184,69 @@ def test_darcy_run_files(tmp_path):
     assert int(first[1]) == int(orc.get("darcy_nijac_last")[0])
     last = binfile.read_bin(str(out / "flow.output00002.bin"), fluid=True)
     assert last.fluid and last.p_f.shape == tuple(int(v) for v in d.num)
+
+
+def grid_case(seed, n=3000, maxiter=200000):
+    """A few thousand spheres on the 40 x 40 x 80 fluid grid of the
+    consolidation workload: 128,000 cells, so the Jacobi launch spans 500
+    blocks of 256 cells and each block waits only for the ~13 blocks within
+    one z layer of its cells (nb_lo > 0 and nb_hi < G - 1 for most blocks)."""
+    d = configs.settling_lattice(n=n, seed=seed, nx=20, ny=20, nz=8, spacing=0.0462, steps=40)
+    dx = 2.1 * 0.011
+    d.num = numpy.array([40, 40, 80], dtype=numpy.uint32)
+    d.L = d.num.astype(numpy.float64) * dx
+    configs.add_top_wall(d, 10e3)
+    # the workload's permeability prefactor, compressibility and tolerance; a
+    # water viscosity keeps the loose packing's (porosity 0.9) pressure
+    # diffusion within the explicit step's stability limit at the DEM dt
+    configs.init_fluid_darcy(d, mu=8.9e-4, rho_f=1000.0, k_c=3.5e-13, beta_f=4.5e-10,
+                             tolerance=1e-8, maxiter=maxiter, bottom_no_flow=True)
+    return d
+
+
+GRID_CASES = {
+    "reference_stop": dict(),
+    "exact_stop": dict(exact=True),
+    "maxiter_mid_ring": dict(maxiter=137),
+}
+
+
+@pytest.mark.parametrize("name", list(GRID_CASES))
+def test_darcy_parity_benchmark_grid(tmp_path, name):
+    """The neighbour-subset waits, the one-iteration-late stop decision and
+    the residual ring of the Jacobi kernel at the benchmark grid size:
+    identical iteration counts and fields within RTOL of the oracle over
+    three fluid steps.  maxiter 137 ends the solve at a check that is not a
+    multiple of 10, after the 64-slot residual ring has wrapped twice."""
+    from sphere_b200.engine import Engine
+    opt = dict(GRID_CASES[name])
+    exact = opt.pop("exact", False)
+    d = grid_case(61, **opt)
+    path = str(tmp_path / "grid.bin")
+    binfile.write_bin(d, path)
+    orc = O.Oracle(path, fluid=True)
+    if exact:
+        orc.set("darcy_exact_stop", numpy.array([1], dtype=numpy.int32))
+    eng = Engine(path, fluid=True, precision="faithful", darcy_exact_stop=exact)
+    iters = []
+    worst = {}
+    for k in range(3):
+        rc_e = eng.step(1)
+        assert orc.step(1) == 0, orc.error()
+        it_o = int(orc.get("darcy_nijac_last")[0])
+        iters.append(it_o)
+        assert int(eng.get("darcy_iters")[0]) == it_o, f"step {k + 1}"
+        assert rc_e == (1 if it_o + 1 == d.maxiter and it_o > 0 else 0), (k, rc_e, it_o)
+        errs = field_errors(eng, orc)
+        for f, e in errs.items():
+            worst[f] = max(worst.get(f, 0.0), e)
+        bad = {f: e for f, e in errs.items() if not e <= RTOL}
+        assert not bad, f"after step {k + 1}: {bad}"
+    print(f"\n{name}: iterations {iters}; worst relative error per field: "
+          + ", ".join(f"{f} {e:.2e}" for f, e in sorted(worst.items())))
+    assert max(iters) >= 40, iters
+    if "maxiter" in opt:
+        assert max(iters) == opt["maxiter"] - 1
+    if exact:
+        assert any(i % 10 for i in iters), iters
+    eng.close()

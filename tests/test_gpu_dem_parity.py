@@ -112,3 +112,119 @@ def test_persistent_refuses_bonds(tmp_path):
         Engine(str(path), step_kernel="persistent")
     with Engine(str(path)) as eng:
         assert eng.step(2) == 0
+
+
+def extra_cases():
+    d = dense(7, n=700); configs.add_top_wall(d, 10e3); d.w_x[0] -= 0.003
+    d.w_sigma0_A = 5e3; d.w_sigma0_f = 50.0
+    yield "sigma0_sinusoid", d, 3
+    d = dense(8, n=700); configs.shear_setup(d, 0.05, 20e3); d.w_x[0] -= 0.003; d.E = 7e8
+    yield "shear_ty2", d, 2
+    d = dense(9, n=700); configs.add_top_wall(d, 20e3); d.w_x[0] -= 0.003
+    d.gamma_n = 50.0; d.gamma_t = 20.0
+    yield "top_wall_viscous_ty2", d, 2
+
+
+@pytest.mark.parametrize("name,data,integrator", list(extra_cases()),
+                         ids=[c[0] for c in extra_cases()])
+@pytest.mark.parametrize("kernel", ["stages", "persistent"])
+def test_step_parity_wall_modulation_and_ty2(tmp_path, name, data, integrator, kernel):
+    """The sinusoidal normal stress of wall 0 (sigma0 + A sin(2 pi f t),
+    src/integration.cuh:383-384) and the two-term Taylor integrator
+    (src/integration.cuh:192-220, 417-427) on both step paths, bit for bit."""
+    from sphere_b200.engine import Engine
+    path = tmp_path / f"{name}.bin"
+    binfile.write_bin(data, path)
+    orc = O.Oracle(str(path), integrator=integrator)
+    eng = Engine(str(path), integrator=integrator, graph_steps=8, step_kernel=kernel)
+    for k, n in enumerate((1, 2, 9, 30)):
+        assert eng.step(n) == 0
+        assert orc.step(n) == 0, orc.error()
+        bad = compare(eng, orc)
+        assert not bad, f"after chunk {k}: {bad}"
+    eng.close()
+
+
+def shear_stress_box(seed):
+    d = dense(seed, n=700)
+    configs.shear_setup(d, 0.0, 20e3)
+    d.w_x[0] -= 0.003
+    d.wmode[0] = 3
+    d.w_tau_x = 5e3
+    return d
+
+
+@pytest.mark.parametrize("precision", ["faithful", "fp64"])
+def test_step_parity_shear_stress_wall(tmp_path, precision):
+    """Wall mode 3: the top particles are driven by the shear stress tau_x
+    plus the effective stress of the fixed moving particles
+    (findShearStressOnFixedMovingParticles + summation,
+    src/integration.cuh:457-484, on the device as k_shear_stress and
+    k_tau_partials), bit for bit.  The fused step refuses wmode 3, so the
+    automatic choice runs the per-stage kernels."""
+    from sphere_b200.engine import Engine, EngineError
+    d = shear_stress_box(10)
+    path = tmp_path / "wmode3.bin"
+    binfile.write_bin(d, path)
+    orc = O.Oracle(str(path), precision=precision)
+    eng = Engine(str(path), precision=precision, graph_steps=8)
+    for k, n in enumerate((1, 2, 9, 30)):
+        assert eng.step(n) == 0
+        assert orc.step(n) == 0, orc.error()
+        bad = compare(eng, orc)
+        assert not bad, f"after chunk {k}: {bad}"
+    moved = eng.get("vel")[:, 0][d.fixvel > 0]
+    assert numpy.abs(moved).max() > 0.0     # the stress moved the top layer
+    eng.close()
+    with pytest.raises(EngineError):
+        Engine(str(path), precision=precision, step_kernel="persistent")
+
+
+def capillary_box(seed):
+    """Model 1 (linear-viscous, no history) with capillary cohesion: pairs
+    within db of contact attract by kappa sqrt(r_a r_b) exp(-delta/lambda)
+    (capillaryCohesion_exp, src/cohesion.cuh:237-277)."""
+    d = dense(seed, n=700, contactmodel=1)
+    d.kappa = 0.05
+    d.db = 0.002
+    d.V_b = 1e-9
+    d.gamma_n = 50.0
+    return d
+
+
+# CUDA's expf and glibc's (the oracle's) may round the capillary exponential
+# differently in the last FP32 bit (CUDA's is documented within 2 ulp), so
+# the capillary case compares the forces to 1e-6 of the largest force and
+# the state to 1e-12 of its largest magnitude; the contact pairs must agree.
+CAP_RTOL_F = 1e-6
+CAP_RTOL_X = 1e-12
+
+
+@pytest.mark.parametrize("precision", ["faithful", "fp64"])
+@pytest.mark.parametrize("kernel", ["stages", "persistent"])
+def test_step_parity_capillary(tmp_path, precision, kernel):
+    from sphere_b200.engine import Engine
+    d = capillary_box(11)
+    path = tmp_path / "capillary.bin"
+    binfile.write_bin(d, path)
+    orc = O.Oracle(str(path), precision=precision)
+    eng = Engine(str(path), precision=precision, graph_steps=8, step_kernel=kernel)
+    for k, n in enumerate((1, 2, 9, 20)):
+        assert eng.step(n) == 0
+        assert orc.step(n) == 0, orc.error()
+        for f, tol in (("force", CAP_RTOL_F), ("torque", CAP_RTOL_F), ("x", CAP_RTOL_X),
+                       ("vel", CAP_RTOL_F), ("angvel", CAP_RTOL_F)):
+            a, b = eng.get(f)[:, :3], orc.get(f)[:, :3]
+            scale = max(float(numpy.abs(b).max()), 1e-300)
+            err = float(numpy.abs(a - b).max()) / scale
+            assert err <= tol, f"after chunk {k}: {f} relative error {err:.3e}"
+        assert numpy.array_equal(eng.get("index"), orc.get("index"))
+    eng.close()
+    # the cohesion acted: without it the first step's forces differ
+    d0 = capillary_box(11)
+    d0.kappa = 0.0
+    path0 = tmp_path / "no_capillary.bin"
+    binfile.write_bin(d0, path0)
+    a, b = O.Oracle(str(path), precision=precision), O.Oracle(str(path0), precision=precision)
+    assert a.step(1) == 0 and b.step(1) == 0
+    assert not numpy.array_equal(a.get("force"), b.get("force"))

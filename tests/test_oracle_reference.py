@@ -12,7 +12,7 @@ from helpers import bonded_packing, compare_states
 from sphere_b200 import binfile, configs
 
 pytestmark = pytest.mark.skipif(
-    not (O.ref_available() or os.path.isdir(O.REF_SRC_DEFAULT)),
+    not (O.ref_available() or O.ref_path("src")),
     reason="reference sources not present")
 
 FIELDS = ("x", "vel", "angvel", "angpos", "force", "torque", "xyzsum", "es", "ev", "p",
@@ -61,12 +61,6 @@ def test_shear_stress_wall_mode(tmp_path):
     run_pair(tmp_path, d)
 
 
-def test_two_term_taylor_is_not_the_reference_default():
-    # The compiled reference integrates with TY3 (src/integration.cuh:10);
-    # TY2 is pinned only through the oracle-vs-engine tests.
-    assert True
-
-
 def test_sigma0_modulation(tmp_path):
     d = configs.settling_lattice(n=400, seed=24, nx=8, ny=8, nz=7, spacing=0.0195, steps=40)
     configs.add_top_wall(d, 10e3)
@@ -77,8 +71,8 @@ def test_sigma0_modulation(tmp_path):
 
 
 def test_reference_fixture_init_1e4(tmp_path):
-    src = "/root/reference/output/init-1e4.output00199.bin"
-    if not os.path.exists(src):
+    src = O.ref_path("output", "init-1e4.output00199.bin")
+    if not src:
         pytest.skip("fixture not present")
     dst = str(tmp_path / "init.bin")
     d = binfile.upgrade_to_215(src, dst)

@@ -73,3 +73,27 @@ def test_rejects_grids_beyond_the_scratch():
     rc = L.sph_sort_cells_noalloc(None, 0, origo, Lv, num, dummy, dummy, dummy, dummy, None)
     assert rc == -8
     assert b"scratch" in L.sph_noalloc_error()
+
+
+def test_rejects_a_crowded_cell():
+    """600 positions in one cell of a 3 x 3 x 3 grid: more than the 512 a
+    warp orders in registers, so the call refuses instead of running a
+    quadratic loop on the GPU."""
+    import torch
+    L = _lib()
+    rng = numpy.random.default_rng(5)
+    n = 600
+    x4 = numpy.zeros((n, 4))
+    x4[:, :3] = rng.uniform(1.05, 1.95, size=(n, 3))
+    x4[:, 3] = 0.01
+    dev = torch.device("cuda", 0)
+    x4_d = torch.from_numpy(x4).to(dev)
+    outs = [torch.zeros((m,), dtype=torch.int32, device=dev) for m in (n, n, 27, 27)]
+    origo = (ctypes.c_double * 3)(0.0, 0.0, 0.0)
+    Lv = (ctypes.c_double * 3)(3.0, 3.0, 3.0)
+    num = (ctypes.c_uint32 * 3)(3, 3, 3)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    rc = L.sph_sort_cells_noalloc(x4_d.data_ptr(), n, origo, Lv, num,
+                                  *(o.data_ptr() for o in outs), stream)
+    assert rc == -8
+    assert b"too coarse" in L.sph_noalloc_error()
