@@ -201,7 +201,19 @@ static void ghost_flux(const orc_state *s, struct orc_darcy *D)
             }
 }
 
-static inline double sphere_volume(double r) { return 4.0 / 3.0 * M_PI * pow(r, 3); }
+/* The reference's pow calls.  Built with ORC_POW_AS_PRODUCTS (the
+ * liboracle_powprod.so variant) they become products, which differ from
+ * pow in the last bit: a probe of how far last-bit differences of a math
+ * library (CUDA's pow on the device against glibc's here) move the solve. */
+#ifdef ORC_POW_AS_PRODUCTS
+#define ORC_CUBE(v) ((v) * (v) * (v))
+#define ORC_SQUARE(v) ((v) * (v))
+#else
+#define ORC_CUBE(v) pow((v), 3)
+#define ORC_SQUARE(v) pow((v), 2)
+#endif
+
+static inline double sphere_volume(double r) { return 4.0 / 3.0 * M_PI * ORC_CUBE(r); }
 
 static double weight_dist(v3 d, double dx, double dy, double dz)
 {
@@ -408,7 +420,7 @@ static void permeabilities(const orc_state *s, struct orc_darcy *D)
                 unsigned c = didx(D, x, y, z);
                 double phi = D->phi[c];
                 if (phi > 0.9999) phi = 0.9999;
-                double k = D->k_c * pow(phi, 3) / pow(1.0 - phi, 2);
+                double k = D->k_c * ORC_CUBE(phi) / ORC_SQUARE(1.0 - phi);
                 D->k[c] = fmin(2.7e-10, k);
             }
 }

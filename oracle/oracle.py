@@ -35,7 +35,7 @@ _U32 = {"cellid", "index", "cellstart", "cellend", "contacts", "bonds"}
 
 def build(ref: bool = True) -> None:
     """Compile liboracle.so and, when the reference sources exist, _ref."""
-    subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
+    subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so", "liboracle_powprod.so"])
     ref_dir = os.environ.get("REF_DIR") or ref_path("src")
     if ref and ref_dir and os.path.isdir(ref_dir):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_DIR={ref_dir}"])
@@ -47,13 +47,17 @@ def _load(path):
     return ctypes.CDLL(path)
 
 
-_lib = None
+_libs = {}
+# the sensitivity probe (pow replaced by products in the Darcy block)
+POWPROD_SO = os.path.join(HERE, "liboracle_powprod.so")
 
 
-def lib():
-    global _lib
+def lib(path=None):
+    path = path or ORACLE_SO
+    _lib = _libs.get(path)
     if _lib is None:
-        _lib = _load(ORACLE_SO)
+        _lib = _load(path)
+        _libs[path] = _lib
         _lib.orc_load.restype = ctypes.c_void_p
         _lib.orc_load.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int, ctypes.c_int,
@@ -105,17 +109,19 @@ class OracleError(RuntimeError):
 class Oracle:
     """The CPU oracle's state for one ``.bin`` input."""
 
-    def __init__(self, path, fluid=False, precision="faithful", integrator=3, nc=32):
+    def __init__(self, path, fluid=False, precision="faithful", integrator=3, nc=32,
+                 lib_path=None):
         status = ctypes.c_int(0)
         prec = {"faithful": 0, "fp64": 1, "true": 1}[precision]
-        self._h = lib().orc_load(os.fsencode(path), int(bool(fluid)), prec,
+        self._L = lib(lib_path)
+        self._h = self._L.orc_load(os.fsencode(path), int(bool(fluid)), prec,
                                  int(integrator), int(nc), ctypes.byref(status))
         if not self._h:
             raise OracleError(f"orc_load failed with status {status.value}")
 
     def close(self):
         if self._h:
-            lib().orc_free(self._h)
+            self._L.orc_free(self._h)
             self._h = None
 
     def __del__(self):
@@ -125,45 +131,45 @@ class Oracle:
             pass
 
     def step(self, n=1):
-        rc = lib().orc_step(self._h, int(n))
+        rc = self._L.orc_step(self._h, int(n))
         return rc
 
     def error(self):
-        return lib().orc_error(self._h).decode()
+        return self._L.orc_error(self._h).decode()
 
     def get(self, name):
-        need = lib().orc_get(self._h, name.encode(), None, 0)
+        need = self._L.orc_get(self._h, name.encode(), None, 0)
         if need < 0:
             raise KeyError(name)
         dtype, shape = _shape(name, need)
         out = numpy.empty(shape, dtype=dtype)
-        rc = lib().orc_get(self._h, name.encode(), out.ctypes.data, out.nbytes)
+        rc = self._L.orc_get(self._h, name.encode(), out.ctypes.data, out.nbytes)
         if rc != 0:
             raise OracleError(f"orc_get({name}) returned {rc}")
         return out
 
     def set(self, name, arr):
         arr = numpy.ascontiguousarray(arr)
-        rc = lib().orc_set(self._h, name.encode(), arr.ctypes.data, arr.nbytes)
+        rc = self._L.orc_set(self._h, name.encode(), arr.ctypes.data, arr.nbytes)
         if rc != 0:
             raise OracleError(f"orc_set({name}) returned {rc}")
 
     def stage(self, which):
-        fn = {"sort": lib().orc_stage_hash_sort_reorder,
-              "topology": lib().orc_stage_topology,
-              "interact": lib().orc_stage_interact}[which]
+        fn = {"sort": self._L.orc_stage_hash_sort_reorder,
+              "topology": self._L.orc_stage_topology,
+              "interact": self._L.orc_stage_interact}[which]
         return fn(self._h)
 
     def write_bin(self, path):
-        return lib().orc_write_bin(self._h, os.fsencode(path))
+        return self._L.orc_write_bin(self._h, os.fsencode(path))
 
     @property
     def np(self):
-        return lib().orc_np(self._h)
+        return self._L.orc_np(self._h)
 
     @property
     def nc(self):
-        return lib().orc_nc(self._h)
+        return self._L.orc_nc(self._h)
 
 
 _ref = None

@@ -98,11 +98,16 @@ def test_darcy_parity(tmp_path, name):
     binfile.write_bin(d, path)
     orc = O.Oracle(path, fluid=True)
     eng = Engine(path, fluid=True, precision="faithful")
+    worst = {}
     for k in range(6):
         assert eng.step(1) == 0
         assert orc.step(1) == 0, orc.error()
         bad = compare(eng, orc)
         assert not bad, f"after step {k + 1}: {bad}"
+        for f, e in field_errors(eng, orc).items():
+            worst[f] = max(worst.get(f, 0.0), e)
+    print(f"\n{name}: worst relative error per field: "
+          + ", ".join(f"{f} {e:.2e}" for f, e in sorted(worst.items())))
     assert int(orc.get("darcy_nijac_last")[0]) > 10
     assert int(eng.get("darcy_iters_total")[0]) == int(orc.get("darcy_nijac_total")[0])
     exact = int(eng.get("darcy_iters_exact")[0])
@@ -210,13 +215,22 @@ GRID_CASES = {
     "maxiter_mid_ring": dict(maxiter=137),
 }
 
+# Beyond RTOL, a field may differ from the oracle by at most SENS_FACTOR
+# times what the oracle itself moves when its pow calls are replaced by
+# products (oracle/liboracle_powprod.so): last-bit changes of the sphere
+# volumes and permeabilities, the size of the difference between CUDA's pow
+# and glibc's.  On this grid the non-converged Jacobi solve (the stop rule is
+# a relative change of 1e-8 per iteration) carries such changes into the
+# pressure at ~1e-9 of its maximum, where the 7 x 7 x 7 cases stay near 1e-11.
+SENS_FACTOR = 10.0
+
 
 @pytest.mark.parametrize("name", list(GRID_CASES))
 def test_darcy_parity_benchmark_grid(tmp_path, name):
     """The neighbour-subset waits, the one-iteration-late stop decision and
     the residual ring of the Jacobi kernel at the benchmark grid size:
-    identical iteration counts and fields within RTOL of the oracle over
-    three fluid steps.  maxiter 137 ends the solve at a check that is not a
+    identical iteration counts and fields within the bound above over three
+    fluid steps.  maxiter 137 ends the solve at a check that is not a
     multiple of 10, after the 64-slot residual ring has wrapped twice."""
     from sphere_b200.engine import Engine
     opt = dict(GRID_CASES[name])
@@ -225,25 +239,30 @@ def test_darcy_parity_benchmark_grid(tmp_path, name):
     path = str(tmp_path / "grid.bin")
     binfile.write_bin(d, path)
     orc = O.Oracle(path, fluid=True)
+    probe = O.Oracle(path, fluid=True, lib_path=O.POWPROD_SO)
     if exact:
-        orc.set("darcy_exact_stop", numpy.array([1], dtype=numpy.int32))
+        for o in (orc, probe):
+            o.set("darcy_exact_stop", numpy.array([1], dtype=numpy.int32))
     eng = Engine(path, fluid=True, precision="faithful", darcy_exact_stop=exact)
     iters = []
-    worst = {}
+    worst, worst_sens = {}, {}
     for k in range(3):
         rc_e = eng.step(1)
         assert orc.step(1) == 0, orc.error()
+        assert probe.step(1) == 0, probe.error()
         it_o = int(orc.get("darcy_nijac_last")[0])
         iters.append(it_o)
         assert int(eng.get("darcy_iters")[0]) == it_o, f"step {k + 1}"
         assert rc_e == (1 if it_o + 1 == d.maxiter and it_o > 0 else 0), (k, rc_e, it_o)
         errs = field_errors(eng, orc)
+        sens = field_errors(probe, orc)
         for f, e in errs.items():
             worst[f] = max(worst.get(f, 0.0), e)
-        bad = {f: e for f, e in errs.items() if not e <= RTOL}
-        assert not bad, f"after step {k + 1}: {bad}"
-    print(f"\n{name}: iterations {iters}; worst relative error per field: "
-          + ", ".join(f"{f} {e:.2e}" for f, e in sorted(worst.items())))
+            worst_sens[f] = max(worst_sens.get(f, 0.0), sens[f])
+        bad = {f: (e, sens[f]) for f, e in errs.items() if not e <= max(RTOL, SENS_FACTOR * sens[f])}
+        assert not bad, f"after step {k + 1}: (error, probe) {bad}"
+    print(f"\n{name}: iterations {iters}; worst relative error per field (probe): "
+          + ", ".join(f"{f} {e:.2e} ({worst_sens[f]:.2e})" for f, e in sorted(worst.items())))
     assert max(iters) >= 40, iters
     if "maxiter" in opt:
         assert max(iters) == opt["maxiter"] - 1
