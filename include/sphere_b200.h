@@ -70,7 +70,10 @@ typedef struct sph_opts {
     const char *output_dir; /* directory for .bin/status/conv outputs; NULL = "output" */
     int step_kernel;      /* 0 automatic (the fused persistent step where it applies),
                              1 per-stage kernels, 2 fused persistent step (error where
-                             it does not apply: bonds, fluid, wmode 3) */
+                             it does not apply: bonds, fluid, wmode 3), 3 per-stage
+                             kernels with the contact search reading its partners
+                             from the neighbour cells staged in shared memory
+                             (same results; slower on the measured workloads) */
     int darcy_exact_stop; /* 1: the Darcy Jacobi loop tests the residual at every
                              iteration and stops at the first that meets the
                              tolerance; 0 (default): the reference's test at

@@ -623,6 +623,8 @@ int ref_write(void *h, const char *path)
     }
     r->dem->transferFromGlobalDeviceMemory();
     r->dem->writebin(path);
+    /* a file output restarts the file clock (device.cu:2556-2600) */
+    r->filetimeclock = 0.0;
     return 0;
 }
 

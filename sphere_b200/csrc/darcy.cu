@@ -1048,7 +1048,7 @@ int Engine::darcy_get(int f, void *dst, size_t bytes)
     if (!darcy) return fail(ST_ARG, "no fluid in this run");
     int64_t need = darcy_field_bytes(f);
     if (need < 0) return fail(ST_ARG, "unknown field");
-    if (!dst || bytes < (size_t)need) return fail(ST_ARG, "destination buffer too small");
+    if ((!dst && need > 0) || bytes < (size_t)need) return fail(ST_ARG, "destination buffer too small");
     DarcyDev &Dd = *darcy;
     const unsigned cb = cells_blocks(Dd.D);
     cudaError_t e = cudaSuccess;

@@ -385,6 +385,60 @@ struct ContactOut {
     double wf0, wf1, wf2, wf3, wf4;   // force on each dynamic wall (walls_force_pp)
 };
 
+// Wall contacts of one particle (contactsearch.cuh:602-701) after its
+// particle contacts, and the results of both into out.
+template <int PREC>
+__device__ __forceinline__ void contact_walls(const DevParams &P, const DevState &S, double4 xa,
+                                              double ra, double4 vel_a, V3 angvel_a, V3 F, V3 T,
+                                              double es_dot, double ev_dot, double p,
+                                              ContactOut &out)
+{
+    // walls beyond nw keep the reference's defaults (the domain faces); the
+    // five walls are unrolled so their state stays in registers
+    const unsigned nw = P.nw;
+    const double4 wnx0 = nw > 0 ? S.wnx[0] : make_double4(0.0f, 0.0f, -1.0f, P.L[2]);
+    const double4 wnx1 = nw > 1 ? S.wnx[1] : make_double4(-1.0f, 0.0f, 0.0f, P.L[0]);
+    const double4 wnx2 = nw > 2 ? S.wnx[2] : make_double4(1.0f, 0.0f, 0.0f, 0.0f);
+    const double4 wnx3 = nw > 3 ? S.wnx[3] : make_double4(0.0f, -1.0f, 0.0f, P.L[1]);
+    const double4 wnx4 = nw > 4 ? S.wnx[4] : make_double4(0.0f, 1.0f, 0.0f, 0.0f);
+    double wf0 = 0.0, wf1 = 0.0, wf2 = 0.0, wf3 = 0.0, wf4 = 0.0;
+    V3 vlin = xyz(vel_a);
+    double dw = wnx0.w - (xa.z + ra);
+    if (dw < 0.0f)
+        wf0 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx0), dw,
+                             nw > 0 ? S.wmvfd[0].y : 0.0);
+    dw = xa.z - ra - P.origo[2];
+    if (dw < 0.0f)
+        (void)wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a,
+                                 mk3(0.0f, 0.0f, 1.0f), dw, 0.0);
+    if (P.periodic == 0) {
+        dw = wnx1.w - (xa.x + ra);
+        if (dw < 0.0f)
+            wf1 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx1), dw,
+                                 nw > 1 ? S.wmvfd[1].y : 0.0);
+        dw = xa.x - ra - wnx2.w;
+        if (dw < 0.0f)
+            wf2 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx2), dw,
+                                 nw > 2 ? S.wmvfd[2].y : 0.0);
+    }
+    if (P.periodic == 0 || P.periodic == 2) {
+        dw = wnx3.w - (xa.y + ra);
+        if (dw < 0.0f)
+            wf3 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx3), dw,
+                                 nw > 3 ? S.wmvfd[3].y : 0.0);
+        dw = xa.y - ra - wnx4.w;
+        if (dw < 0.0f)
+            wf4 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx4), dw,
+                                 nw > 4 ? S.wmvfd[4].y : 0.0);
+    }
+    out.F = F;
+    out.T = T;
+    out.es_dot = es_dot;
+    out.ev_dot = ev_dot;
+    out.p = p;
+    out.wf0 = wf0; out.wf1 = wf1; out.wf2 = wf2; out.wf3 = wf3; out.wf4 = wf4;
+}
+
 // Contact search + forces of sorted particle k (topology and interact of
 // the reference, walls included).  srow is the thread's slot scratch in
 // shared memory (entry i at srow[i * B + t]: the partner's original index).
@@ -532,51 +586,7 @@ __device__ __forceinline__ bool contact_particle(const DevParams &P, const DevSt
         }
     }
 
-    // --- walls (contactsearch.cuh:602-701) ---
-    // walls beyond nw keep the reference's defaults (the domain faces); the
-    // five walls are unrolled so their state stays in registers
-    const unsigned nw = P.nw;
-    const double4 wnx0 = nw > 0 ? S.wnx[0] : make_double4(0.0f, 0.0f, -1.0f, P.L[2]);
-    const double4 wnx1 = nw > 1 ? S.wnx[1] : make_double4(-1.0f, 0.0f, 0.0f, P.L[0]);
-    const double4 wnx2 = nw > 2 ? S.wnx[2] : make_double4(1.0f, 0.0f, 0.0f, 0.0f);
-    const double4 wnx3 = nw > 3 ? S.wnx[3] : make_double4(0.0f, -1.0f, 0.0f, P.L[1]);
-    const double4 wnx4 = nw > 4 ? S.wnx[4] : make_double4(0.0f, 1.0f, 0.0f, 0.0f);
-    double wf0 = 0.0, wf1 = 0.0, wf2 = 0.0, wf3 = 0.0, wf4 = 0.0;
-    V3 vlin = xyz(vel_a);
-    double dw = wnx0.w - (xa.z + ra);
-    if (dw < 0.0f)
-        wf0 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx0), dw,
-                             nw > 0 ? S.wmvfd[0].y : 0.0);
-    dw = xa.z - ra - P.origo[2];
-    if (dw < 0.0f)
-        (void)wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a,
-                                 mk3(0.0f, 0.0f, 1.0f), dw, 0.0);
-    if (P.periodic == 0) {
-        dw = wnx1.w - (xa.x + ra);
-        if (dw < 0.0f)
-            wf1 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx1), dw,
-                                 nw > 1 ? S.wmvfd[1].y : 0.0);
-        dw = xa.x - ra - wnx2.w;
-        if (dw < 0.0f)
-            wf2 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx2), dw,
-                                 nw > 2 ? S.wmvfd[2].y : 0.0);
-    }
-    if (P.periodic == 0 || P.periodic == 2) {
-        dw = wnx3.w - (xa.y + ra);
-        if (dw < 0.0f)
-            wf3 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx3), dw,
-                                 nw > 3 ? S.wmvfd[3].y : 0.0);
-        dw = xa.y - ra - wnx4.w;
-        if (dw < 0.0f)
-            wf4 = wall_law<PREC>(P, F, T, es_dot, ev_dot, p, ra, vlin, angvel_a, xyz(wnx4), dw,
-                                 nw > 4 ? S.wmvfd[4].y : 0.0);
-    }
-    out.F = F;
-    out.T = T;
-    out.es_dot = es_dot;
-    out.ev_dot = ev_dot;
-    out.p = p;
-    out.wf0 = wf0; out.wf1 = wf1; out.wf2 = wf2; out.wf3 = wf3; out.wf4 = wf4;
+    contact_walls<PREC>(P, S, xa, ra, vel_a, angvel_a, F, T, es_dot, ev_dot, p, out);
     return true;
 }
 
@@ -657,20 +667,30 @@ struct StepClock {
     double tau_eff_x;
 };
 
+// The inputs of one particle's integration step (its state before the step
+// and the forces of the step).
+struct IntegrateIn {
+    double4 force, torque, x, vel, angvel, angpos, xyzsum, acc0, angacc0;
+    float4 x_ref;      // position at the last neighbour-list build
+    uint32_t cell;     // cell of the current sort
+};
+
 // integrate, src/integration.cuh:14-305 (TY3 default, TY2 selectable), for
-// sorted particle k with its force and torque, followed by the cell hash of
-// the new position (src/sorting.cuh:7-51).  Reads the current state from S
-// and writes the new x, vel, angvel (and their FP32 copies when vel_f_out
-// is set) to the *_out arrays -- S's own arrays for the in-place kernel, the
-// other buffer of a ping-pong pair for the fused step.  Raises *resort_flag
-// when the cell changed and *nl_flag when the particle left its
-// neighbour-list skin.  Returns false after raising an outside-grid error.
-__device__ __forceinline__ bool integrate_particle(const DevParams &P, const DevState &S, unsigned k,
-                                                   double4 force, double4 torque, const StepClock &clk,
-                                                   double4 *x_out, double4 *vel_out,
-                                                   double4 *angvel_out, float4 *vel_f_out,
-                                                   float4 *angvel_f_out, int *resort_flag,
-                                                   int *nl_flag)
+// sorted particle k with the inputs `in` (acc0 / angacc0 are read only
+// after the first step, as the reference does), followed by the cell hash
+// of the new position (src/sorting.cuh:7-51).  Writes the new x, vel,
+// angvel (and their FP32 copies when vel_f_out is set) to the *_out arrays
+// -- S's own arrays for the in-place kernel, the other buffer of a ping-pong
+// pair for the fused step -- and acc, angacc, angpos, xyzsum, cell_new to S.
+// Raises *resort_flag when the cell changed and *nl_flag when the particle
+// left its neighbour-list skin.  Returns false after raising an outside-grid
+// error.
+__device__ __forceinline__ bool integrate_values(const DevParams &P, const DevState &S, unsigned k,
+                                                 const IntegrateIn &in, const StepClock &clk,
+                                                 double4 *x_out, double4 *vel_out,
+                                                 double4 *angvel_out, float4 *vel_f_out,
+                                                 float4 *angvel_f_out, int *resort_flag,
+                                                 int *nl_flag)
 {
     const long long iter = clk.iter;
     const double t_current = clk.t_current;
@@ -683,9 +703,10 @@ __device__ __forceinline__ bool integrate_particle(const DevParams &P, const Dev
         else if (t_current >= 15.0 && vs == 2) change_velocity_state = -1;
     }
     const double velocity_factor = 10.0;
-    double4 angpos = S.angpos[k];
-    double4 x = S.x[k], vel = S.vel[k], angvel = S.angvel[k];
-    double4 xyzsum = S.xyzsum[k];
+    const double4 force = in.force, torque = in.torque;
+    double4 angpos = in.angpos;
+    double4 x = in.x, vel = in.vel, angvel = in.angvel;
+    double4 xyzsum = in.xyzsum;
     int wall0mode = 0;
     double wall0mass = 0.0;
     if (P.nw > 0) {
@@ -696,8 +717,8 @@ __device__ __forceinline__ bool integrate_particle(const DevParams &P, const Dev
     if (P.nw > 0 && wall0mode == 3) tau_eff_x = clk.tau_eff_x;
     double4 acc0 = make_double4(0, 0, 0, 0), angacc0 = make_double4(0, 0, 0, 0);
     if (iter != 0) {
-        acc0 = S.acc[k];
-        angacc0 = S.angacc[k];
+        acc0 = in.acc0;
+        angacc0 = in.angacc0;
     }
     double radius = x.w;
     double dt = P.dt;
@@ -812,14 +833,43 @@ __device__ __forceinline__ bool integrate_particle(const DevParams &P, const Dev
     }
     unsigned c = ((unsigned)iz * P.num[1]) * P.num[0] + (unsigned)iy * P.num[0] + (unsigned)ix;
     S.cell_new[k] = c;
-    if (c != S.cell_of[k]) *resort_flag = 1;
+    if (c != in.cell) *resort_flag = 1;
     // neighbour lists stay exact while every particle is within 0.45 skin
     // of its position at the build
-    float4 xr = S.x_ref[k];
+    const float4 xr = in.x_ref;
     double ddx = x_new.x - (double)xr.x, ddy = x_new.y - (double)xr.y, ddz = x_new.z - (double)xr.z;
     double lim = 0.45 * P.skin;
     if (ddx * ddx + ddy * ddy + ddz * ddz > lim * lim) *nl_flag = 1;
     return true;
+}
+
+// integrate_values for sorted particle k with its state read from S and the
+// given force and torque.
+__device__ __forceinline__ bool integrate_particle(const DevParams &P, const DevState &S, unsigned k,
+                                                   double4 force, double4 torque, const StepClock &clk,
+                                                   double4 *x_out, double4 *vel_out,
+                                                   double4 *angvel_out, float4 *vel_f_out,
+                                                   float4 *angvel_f_out, int *resort_flag,
+                                                   int *nl_flag)
+{
+    IntegrateIn in;
+    in.force = force;
+    in.torque = torque;
+    in.angpos = S.angpos[k];
+    in.x = S.x[k];
+    in.vel = S.vel[k];
+    in.angvel = S.angvel[k];
+    in.xyzsum = S.xyzsum[k];
+    in.acc0 = make_double4(0, 0, 0, 0);
+    in.angacc0 = make_double4(0, 0, 0, 0);
+    if (clk.iter != 0) {
+        in.acc0 = S.acc[k];
+        in.angacc0 = S.angacc[k];
+    }
+    in.cell = S.cell_of[k];
+    in.x_ref = S.x_ref[k];
+    return integrate_values(P, S, k, in, clk, x_out, vel_out, angvel_out, vel_f_out, angvel_f_out,
+                            resort_flag, nl_flag);
 }
 
 }  // namespace sphb

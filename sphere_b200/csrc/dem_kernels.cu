@@ -4,6 +4,7 @@
 // operation order and rounding (the reference is built with --fmad=false,
 // src/CMakeLists.txt:25).  One thread per particle in sorted order.
 #include "dem_device.cuh"
+#include "contacts_staged.cuh"
 #include "dem_launch.h"
 #include "reduce_device.cuh"
 
@@ -246,9 +247,44 @@ __global__ void k_hash(DevParams P, DevState S)
 // ---------------------------------------------------------------------
 static inline unsigned blocks_for(unsigned n, unsigned b) { return (n + b - 1) / b; }
 
-cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cudaStream_t st)
+// SPHB_STAGED_MINB resident blocks per SM: each block's dynamic shared memory
+// leaves room for the others (228 KB per SM, 1 KB reserved per block, and the
+// block's static shared memory), at most 227 KB per block.
+void staged_contact_shape(unsigned nc, size_t per_particle, size_t &smem, unsigned &cap)
+{
+    size_t budget = 233472 / SPHB_STAGED_MINB - 1024 - 512;
+    if (budget > 232448 - 512) budget = 232448 - 512;
+    const size_t fixed = stage_smem_bytes(nc, SPHB_STAGED_B, 0, per_particle);
+    if (!SPHB_STAGED_ON) {
+        cap = 0;
+        smem = fixed;
+        return;
+    }
+    cap = fixed + 256 * per_particle > budget ? 256u : (unsigned)((budget - fixed) / per_particle);
+    smem = stage_smem_bytes(nc, SPHB_STAGED_B, cap, per_particle);
+}
+
+cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cudaStream_t st,
+                            int staged)
 {
     if (P.np == 0) return cudaSuccess;
+    if (P.contactmodel == 2 && staged) {
+        size_t smem;
+        unsigned cap;
+        staged_contact_shape(P.nc, stage_bytes_per_particle<0>(), smem, cap);
+        static size_t attr = 0;
+        if (attr < smem) {
+            cudaFuncSetAttribute(k_contacts_staged<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+            cudaFuncSetAttribute(k_contacts_staged<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+            attr = smem;
+        }
+        dim3 grid(blocks_for(P.np, SPHB_STAGED_B));
+        if (prec == 0) k_contacts_staged<0><<<grid, SPHB_STAGED_B, smem, st>>>(P, S, cap);
+        else k_contacts_staged<1><<<grid, SPHB_STAGED_B, smem, st>>>(P, S, cap);
+        return cudaGetLastError();
+    }
     const unsigned B = SPHB_CONTACT_B;
     dim3 grid(blocks_for(P.np, B));
     if (P.contactmodel == 2) {

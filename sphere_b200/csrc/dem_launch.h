@@ -8,10 +8,18 @@
 
 namespace sphb {
 
-// prec: 0 faithful FP64 (FP32 lengths), 1 FP64.
-cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cudaStream_t st);
+// prec: 0 faithful FP64 (FP32 lengths), 1 FP64.  staged = 1: contact model 2
+// reads its partners from the neighbour cells staged in shared memory
+// (k_contacts_staged); 0 walks the neighbour lists through global memory
+// (k_contacts).
+cudaError_t launch_contacts(const DevParams &P, const DevState &S, int prec, cudaStream_t st,
+                            int staged = 0);
 // mixed precision: FP64 overlaps, FP32 contact laws, FP64 accumulation
-cudaError_t launch_contacts_mixed(const DevParams &P, const DevState &S, cudaStream_t st);
+cudaError_t launch_contacts_mixed(const DevParams &P, const DevState &S, cudaStream_t st,
+                                  int staged = 0);
+// Shared memory of the staged contact kernel: bytes per block and the
+// staging capacity (particles) for nc slots per particle.
+void staged_contact_shape(unsigned nc, size_t per_particle, size_t &smem, unsigned &cap);
 cudaError_t launch_bonds(const DevParams &P, const DevState &S, int prec, double4 *bond_f,
                          double4 *bond_t, cudaStream_t st);
 // shear-stress reduction (wmode 3), then one kernel: integration, wall

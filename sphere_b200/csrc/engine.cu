@@ -293,8 +293,9 @@ cudaError_t Engine::enqueue_stage(int stage)
     switch (stage) {
     case 0: return launch_resort(P, S, S.perm_scratch, 0, stream, 1);
     case 1:
-        if (precision == SPH_PREC_MIXED) return launch_contacts_mixed(P, S, stream);
-        return launch_contacts(P, S, prec, stream);
+        if (precision == SPH_PREC_MIXED)
+            return launch_contacts_mixed(P, S, stream, step_kernel == 3);
+        return launch_contacts(P, S, prec, stream, step_kernel == 3);
     case 2: return launch_bonds(P, S, prec, bond_f, bond_t, stream);
     case 3: return enqueue_fluid();
     case 4: return launch_integrate(P, S, stream);
@@ -480,7 +481,7 @@ int Engine::get(int f, void *dst, size_t bytes)
 {
     int64_t need = field_bytes(f);
     if (need < 0) return fail(ST_ARG, "unknown field");
-    if (!dst || bytes < (size_t)need) return fail(ST_ARG, "destination buffer too small");
+    if ((!dst && need > 0) || bytes < (size_t)need) return fail(ST_ARG, "destination buffer too small");
     size_t n = hs.np;
     cudaError_t e = cudaSuccess;
     auto d2h = [&](const void *src, size_t b) {
@@ -830,6 +831,7 @@ static int open_common(std::unique_ptr<Engine> &eng, const sph_opts *opts)
     e.darcy_exact_stop = o.darcy_exact_stop ? 1 : 0;
     e.inject = (uint32_t)o.inject_timeout;
     e.outdir = o.output_dir ? o.output_dir : "output";
+    if (e.step_kernel < 0 || e.step_kernel > 3) return e.fail(sphb::ST_ARG, "unknown step_kernel");
     if (e.precision != SPH_PREC_FAITHFUL && e.precision != SPH_PREC_FP64 &&
         e.precision != SPH_PREC_MIXED)
         return e.fail(sphb::ST_ARG, "unknown precision mode");

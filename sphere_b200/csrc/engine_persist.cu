@@ -47,7 +47,7 @@ cudaError_t launch_refresh_f(const DevParams &P, const DevState &S, cudaStream_t
 
 bool Engine::persist_eligible() const
 {
-    if (step_kernel == 1) return false;
+    if (step_kernel == 1 || step_kernel == 3) return false;
     // the fused step covers dry runs without bonds or the shear-stress wall
     return !hs.fluid && hs.nb0 == 0 && !(hs.nw > 0 && hs.wmode[0] == 3) && hs.np > 0;
 }

@@ -1141,7 +1141,7 @@ int Engine::ns_get(int f, void *dst, size_t bytes)
 {
     const int64_t need = ns_field_bytes(f);
     if (need < 0) return fail(ST_ARG, "field not available with the Navier-Stokes solver");
-    if (!dst || bytes < (size_t)need) return fail(ST_ARG, "destination buffer too small");
+    if ((!dst && need > 0) || bytes < (size_t)need) return fail(ST_ARG, "destination buffer too small");
     NSDev &D = *ns;
     const NSParams &N = D.N;
     const size_t nc = hs.ncells();

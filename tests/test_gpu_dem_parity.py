@@ -60,10 +60,11 @@ def cases():
 
 @pytest.mark.parametrize("name,data", list(cases()), ids=[c[0] for c in cases()])
 @pytest.mark.parametrize("precision", ["faithful", "fp64"])
-@pytest.mark.parametrize("kernel", ["stages", "persistent"])
+@pytest.mark.parametrize("kernel", ["stages", "persistent", "stages_staged"])
 def test_step_parity(tmp_path, name, data, precision, kernel):
-    """Both step paths -- the per-stage kernels and the fused persistent
-    kernel -- against the oracle, bit for bit."""
+    """Every step path -- the per-stage kernels, the fused persistent kernel
+    and the per-stage kernels with the contact search reading the neighbour
+    cells staged in shared memory -- against the oracle, bit for bit."""
     from sphere_b200.engine import Engine
     path = tmp_path / f"{name}.bin"
     binfile.write_bin(data, path)
