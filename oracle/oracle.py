@@ -197,6 +197,9 @@ def ref_lib():
         _ref.ref_overlaps.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_long]
         _ref.ref_overlaps.restype = ctypes.c_long
+        _ref.ref_render.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                    ctypes.c_uint, ctypes.c_uint, ctypes.c_void_p]
+        _ref.ref_render.restype = ctypes.c_int
     return _ref
 
 
@@ -229,6 +232,16 @@ class Reference:
         if n != slices:
             raise OracleError(f"porosity printed {n} of {slices} lines")
         return z, p
+
+    def render(self, method=1, max_val=1.0e3, lower_cutoff=0.0, width=800, height=800):
+        """DEM::render's image of the current state (`sphere --render`):
+        height x width x 4 bytes (RGBA; alpha untouched, 0)."""
+        img = numpy.zeros((height, width, 4), dtype=numpy.uint8)
+        rc = ref_lib().ref_render(self._h, int(method), float(max_val), float(lower_cutoff),
+                                  int(width), int(height), img.ctypes.data)
+        if rc != 0:
+            raise OracleError(f"render method {method} not understood")
+        return img
 
     def overlaps(self):
         """DEM::findOverlaps: (pairs M x 2, separations M)."""

@@ -72,6 +72,18 @@ template <class F> static void launch3(dim3 grid, dim3 block, F f)
             }
 }
 
+/* The reference's ray-tracing kernels (src/raytracer.cuh:14-275), compiled
+ * from the reference's file in a unit of their own (oracle/Makefile). */
+void imageInit(unsigned char *dev_img, const unsigned int pixels);
+void rayInitPerspective(float4 *dev_ray_origo, float4 *dev_ray_direction, const float4 eye,
+                        const unsigned int width, const unsigned int height);
+void rayIntersectSpheres(const float4 *dev_ray_origo, const float4 *dev_ray_direction,
+                         const Float4 *dev_x, unsigned char *dev_img);
+void rayIntersectSpheresColormap(const float4 *dev_ray_origo, const float4 *dev_ray_direction,
+                                 const Float4 *dev_x, const Float4 *dev_vel, const Float *dev_linarr,
+                                 const float max_val, const float lower_cutoff,
+                                 unsigned char *dev_img);
+
 static unsigned idiv_up(unsigned a, unsigned b) { return (a % b != 0) ? (a / b + 1) : (a / b); }
 
 /* ---- host stand-ins for the device-memory members of device.cu ---- */
@@ -785,6 +797,79 @@ long ref_overlaps(void *h, unsigned *pairs, double *delta, long cap)
         delta[q] = d[q];
     }
     return (long)ij.size();
+}
+
+/* DEM::render and DEM::cameraInit (src/raytracer.cuh:278-520): the camera
+ * from the grid and the largest particle coordinates, the rays of
+ * rayInitPerspective, then rayIntersectSpheres (method 0) or
+ * rayIntersectSpheresColormap with the method's per-particle values, each
+ * kernel run one thread at a time.  img receives width * height RGBA bytes.
+ * The kernels' bound checks let the thread with index width * height run;
+ * the ray and image buffers carry one spare entry for it. */
+int ref_render(void *h, int method, float maxval, float lower_cutoff, unsigned width,
+               unsigned height, unsigned char *img)
+{
+    RefRun *r = (RefRun *)h;
+    DEM &d = *r->dem;
+    d.transferFromGlobalDeviceMemory();
+    const unsigned np = d.np;
+    const unsigned pixels = width * height;
+    const unsigned tpb = 256, bpg = idiv_up(pixels, tpb);
+    std::vector<unsigned char> dev_img(4 * ((size_t)pixels + 1), 0);
+    std::vector<float4> ray_o((size_t)pixels + 1), ray_d((size_t)pixels + 1);
+    launch(bpg, tpb, [&] { imageInit(dev_img.data(), pixels); });
+    /* DEM::render */
+    const float imgw = d.grid.L[0] * 1.35f;
+    const Float3 maxpos = d.maxPos();
+    const float3 lookat = make_float3(maxpos.x, maxpos.y, maxpos.z) / 2.0f;
+    const float3 eye = make_float3(d.grid.L[0] * 2.3f, d.grid.L[1] * -5.0f, d.grid.L[2] * 1.3f);
+    /* DEM::cameraInit */
+    {
+        const float hw_ratio = height / width;
+        const float4 imgplane = make_float4(-0.5f * imgw, 0.5f * imgw, -0.5f * imgw * hw_ratio,
+                                            0.5f * imgw * hw_ratio);
+        const float3 view = eye - lookat;
+        const float3 up = make_float3(0.0f, 0.0f, 1.0f);
+        const float3 w = -view / length(view);
+        const float3 u = cross(up, w) / length(cross(up, w));
+        const float3 v = cross(w, u);
+        const float dd = length(view) * 0.8f;
+        const float3 light = normalize(-1.0f * eye * make_float3(1.0f, 0.2f, 0.6f));
+        devC_u = u;
+        devC_v = v;
+        devC_w = w;
+        devC_eye = eye;
+        devC_imgplane = imgplane;
+        devC_d = dd;
+        devC_light = light;
+        devC_pixels = pixels;
+    }
+    devC_np = np;
+    launch(bpg, tpb, [&] {
+        rayInitPerspective(ray_o.data(), ray_d.data(), make_float4(eye.x, eye.y, eye.z, 0.0f),
+                           width, height);
+    });
+    if (method == 0) {
+        launch(bpg, tpb, [&] { rayIntersectSpheres(ray_o.data(), ray_d.data(), d.dev_x, dev_img.data()); });
+    } else {
+        std::vector<Float> linarr(np ? np : 1);
+        const Float *vals = linarr.data();
+        for (unsigned i = 0; i < np; ++i) {
+            const Float4 &ve = d.k.vel[i], &w = d.k.angvel[i], &xs = d.k.xyzsum[i], &ap = d.k.angpos[i];
+            if (method == 2) linarr[i] = sqrt(ve.x * ve.x + ve.y * ve.y + ve.z * ve.z);
+            else if (method == 3) linarr[i] = sqrt(w.x * w.x + w.y * w.y + w.z * w.z);
+            else if (method == 4) linarr[i] = xs.x;
+            else if (method == 5) linarr[i] = sqrt(ap.x * ap.x + ap.y * ap.y + ap.z * ap.z);
+        }
+        if (method == 1) vals = d.dev_p;
+        else if (method < 1 || method > 5) return -1;
+        launch(bpg, tpb, [&] {
+            rayIntersectSpheresColormap(ray_o.data(), ray_d.data(), d.dev_x, d.dev_vel, vals, maxval,
+                                        lower_cutoff, dev_img.data());
+        });
+    }
+    std::memcpy(img, dev_img.data(), 4 * (size_t)pixels);
+    return 0;
 }
 
 void ref_close(void *h)

@@ -11,10 +11,10 @@ of src/colorbar.h.  All of it is IEEE single precision, as numpy float32
 evaluates it; vector lengths and normalisation use sqrt and a division
 (the host form of the reference's vector helpers).
 
-Parity is pinned by analytic cases in tests/test_render_oracle.py (a
-sphere on the optical axis, the camera basis, the colour map), not by the
-reference itself: its renderer cannot be built for the host (its driver is
-CUDA host code with kernel launches and constant-memory copies).
+Parity is pinned against the reference's own kernels (rayInitPerspective,
+rayIntersectSpheres, rayIntersectSpheresColormap of src/raytracer.cuh,
+compiled for the host in oracle/_ref and run one thread at a time) and by
+analytic cases, in tests/test_render_oracle.py.
 """
 from __future__ import annotations
 

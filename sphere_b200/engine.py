@@ -35,7 +35,7 @@ _I64 = {"iter", "velocity_state", "darcy_iters", "darcy_iters_total", "darcy_ite
 
 STATUS = {
     0: "ok", 1: "Darcy solve did not converge", -1: "file error", -2: "version",
-    -3: "input check failed", -4: "CUDA error", -5: "particle outside the grid",
+    -3: "input check failed", -4: "CUDA error", -5: "particle outside the grid or a non-finite value",
     -6: "contact capacity exceeded", -7: "unsupported input", -8: "bad argument",
     -9: "device wait timed out",
 }

@@ -121,3 +121,29 @@ def test_extrapolation_start():
     assert numpy.mean(it_extra[-40:]) <= numpy.mean(it_plain[-40:])
     plain.close()
     extra.close()
+
+
+def test_learned_start_against_extrapolation_alone():
+    """What the trained network adds to its extrapolation in time
+    (warm_start 1 against 2, same tolerance and stop rule, exact iteration
+    counts over the second half of the run).  On the consolidation runs
+    measured so far it adds nothing: the extrapolation alone already halves
+    the iterations of the plain start, and the network's corrected guess,
+    when it wins the first-residual comparison, converges no faster.  The
+    comparison with the fallback bounds what the network can cost: at most
+    5 % more iterations than the extrapolation alone."""
+    from sphere_b200.engine import Engine
+    d = _consolidation(seed=61)
+    runs = {}
+    for mode in (0, 1, 2):
+        e = Engine(d, fluid=True, warm_start=mode)
+        it = []
+        for step in range(120):
+            assert e.step(1) == 0
+            it.append(int(e.get("darcy_iters_exact")[0]))
+        runs[mode] = float(numpy.mean(it[60:]))
+        e.close()
+    print("iterations per solve: plain", runs[0], "learned", runs[1], "extrapolation", runs[2],
+          "network gain", runs[2] / max(runs[1], 1e-9))
+    assert runs[2] < runs[0] and runs[1] < runs[0]
+    assert runs[1] <= 1.05 * runs[2]

@@ -1,12 +1,46 @@
-"""The renderer's CPU restatement (oracle/render_oracle.py) on cases whose
-answer is known without it: the camera basis, a single sphere seen on the
-optical axis, the colour map's end points, the cut-off and fixed-particle
-rules."""
+"""The renderer's CPU restatement (oracle/render_oracle.py) against the
+reference's own ray-tracing kernels (src/raytracer.cuh, compiled for the
+host in oracle/_ref), pixel for pixel, and on cases whose answer is known
+without either: the camera basis, a single sphere seen on the optical axis,
+the colour map's end points, the cut-off and fixed-particle rules."""
 import math
+import os
 
 import numpy
+import pytest
 
+import oracle as O
 import render_oracle as R
+
+CASES = [(0, 1e3, 0.0), (1, 50.0, 0.0), (2, 0.05, 0.0), (3, 1.0, 0.0), (4, 1e-4, 0.0),
+         (5, 1e-3, 0.0), (2, 0.05, 0.01)]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="host build of the reference not present")
+def test_oracle_matches_reference_kernels(tmp_path):
+    """rayInitPerspective, rayIntersectSpheres and rayIntersectSpheresColormap
+    of the reference, run one thread at a time on a stepped packing, give the
+    restatement's image for every colouring method, square and tall images,
+    with and without the cut-off."""
+    from sphere_b200 import binfile, configs
+    d = configs.settling_lattice(n=300, seed=101, nx=7, ny=7, nz=7, spacing=0.0195, steps=0)
+    d.fixvel[:10] = 1.0
+    path = os.path.join(str(tmp_path), "rt.bin")
+    binfile.write_bin(d, path)
+    ref = O.Reference(path)
+    assert ref.step(60) == 0
+    s = {k: ref.get(k) for k in ("x", "vel", "angvel", "xyzsum", "angpos", "p")}
+    for method, max_val, cutoff in CASES:
+        val = R.method_values(method, s["x"], s["vel"], s["angvel"], s["xyzsum"], s["angpos"],
+                              s["p"])
+        for w, h in ((64, 64), (48, 96)):
+            img = ref.render(method, max_val, cutoff, w, h)
+            want = R.render(s["x"], s["vel"], d.L, w, h, method=method, val=val,
+                            max_val=max_val, lower_cutoff=cutoff)
+            assert (want[:, :, :3] != 255).any()
+            bad = numpy.argwhere((img[:, :, :3] != want[:, :, :3]).any(axis=2))
+            assert len(bad) == 0, (method, w, h, bad[:5])
+    ref.close()
 
 
 def test_camera_basis():
