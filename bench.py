@@ -144,7 +144,7 @@ def measure(d, precision, args, flush):
     from sphere_b200.engine import Engine
 
     n = d.np
-    eng = Engine(d, precision=precision, graph_steps=INTERVAL)
+    eng = Engine(d, precision=precision, graph_steps=INTERVAL, step_kernel=args.step_kernel)
     for _ in range(args.warmup):
         eng.step(INTERVAL)
     torch.cuda.synchronize()
@@ -640,6 +640,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["faithful", "fp64", "mixed"])
+    ap.add_argument("--step-kernel", default="auto",
+                    choices=["auto", "stages", "persistent", "stages_staged"],
+                    help="step path of the shear leg: automatic (autotuned), the per-stage "
+                         "kernels, the fused persistent kernel, or the per-stage kernels with "
+                         "the contact search reading neighbour cells staged in shared memory")
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--ref-sample", type=int, default=INTERVAL,

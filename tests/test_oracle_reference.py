@@ -156,3 +156,23 @@ def test_reference_ns_reproduces_golden_fixture():
                 assert numpy.array_equal(ref.get(name), gold[key]), key
     assert int(gold["ns_nijac_last@3"][0]) > 10
     ref.close()
+
+
+def test_capillary_cohesion(tmp_path):
+    """Model 1 with capillary cohesion (capillaryCohesion_exp,
+    src/cohesion.cuh:237-277, called for pairs within db of contact,
+    src/contactsearch.cuh:91-186): oracle and reference bit for bit, and the
+    cohesion changes the forces."""
+    d = configs.settling_lattice(n=500, seed=25, nx=8, ny=8, nz=8, spacing=0.0195, steps=40,
+                                 contactmodel=1)
+    d.kappa = 0.05
+    d.db = 0.002
+    d.V_b = 1e-9
+    d.gamma_n = 50.0
+    orc, _ = run_pair(tmp_path, d)
+    d.kappa = 0.0
+    path = str(tmp_path / "dry.bin")
+    binfile.write_bin(d, path)
+    dry = O.Oracle(path)
+    assert dry.step(20) == 0
+    assert not numpy.array_equal(dry.get("force"), orc.get("force"))
