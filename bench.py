@@ -18,9 +18,11 @@ memory, advances INTERVAL DEM steps and reads the state back (positions,
 velocities, angular velocities, forces, torques).
 
 `python bench.py --impl reference` times the reference algorithm on the host
-cores instead: the CPU restatement of the reference's step (the oracle,
-OpenMP over all host threads; sphere has no CPU DEM path of its own) on a
-bounded sample of the same workload.
+cores instead, on a bounded sample of the same workload: the reference's own
+kernels compiled for the host (oracle/_ref, one thread; sphere has no CPU DEM
+path of its own), or where that build is absent the CPU restatement of the
+reference's step (the oracle, OpenMP over all host threads).  The engine's
+line carries the latter as `cpu_baseline`.
 """
 from __future__ import annotations
 
@@ -586,39 +588,61 @@ def cpu_baseline(d, sample_steps=3):
             "sample": f"{sample_steps} DEM steps of the N={d.np} workload after 1 warm-up step"}
 
 
+# DEM steps per benchmark step of the reference arm when it runs the
+# reference's own kernels built for the host: they run one thread at a time
+# (about 0.2 s per DEM step of this workload on one core), so a benchmark step
+# of INTERVAL DEM steps would make a 30-step run last ten minutes
+REF_BUILD_SAMPLE = 10
+
+
 def run_reference(args):
+    """The reference arm: the reference's own FP64 step on the host cores.
+    Where the reference's kernels were compiled for the host (oracle/_ref:
+    sorting.cuh, contactsearch.cuh, contactmodels.cuh, integration.cuh,
+    ... driven one thread at a time, the reference having no CPU DEM path of
+    its own), those; otherwise the oracle's restatement of them on all host
+    threads.  Each benchmark step times a bounded sample of DEM steps of the
+    same workload; the metric is per particle and DEM step."""
     n = args.particles
     d = workload(n)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import tempfile
     import oracle as O
     from sphere_b200 import binfile
+    kind = "reference" if O.ref_available() else "port"
+    sample_steps = args.ref_sample or (REF_BUILD_SAMPLE if kind == "reference" else INTERVAL)
     times = []
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "w.bin")
         binfile.write_bin(d, path)
-        orc = O.Oracle(path, precision="faithful")
+        runner = O.Reference(path) if kind == "reference" else O.Oracle(path, precision="faithful")
         # warm-up steps: one DEM step each (the CPU code has no state a
-        # longer warm-up would prepare); timed steps: INTERVAL DEM steps
-        # each, as in the engine arm
+        # longer warm-up would prepare)
         for _ in range(args.warmup):
-            orc.step(1)
+            runner.step(1)
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            rc = orc.step(args.ref_sample)
+            rc = runner.step(sample_steps)
             t1 = time.perf_counter()
             if rc:
-                raise RuntimeError(orc.error())
+                raise RuntimeError(f"reference step failed with status {rc}")
             times.append(t1 - t0)
-        orc.close()
+        runner.close()
     total = float(numpy.sum(times))
-    value = n * args.ref_sample * args.steps / total
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    sample = (f"{args.ref_sample} DEM steps of the N={n} workload per benchmark step: the oracle "
-              f"(a C restatement of the reference's FP64 step, pinned bit-exact against the "
-              f"reference's own kernels built for the host), OpenMP on {cores} threads")
+    value = n * sample_steps * args.steps / total
+    if kind == "reference":
+        cores = 1
+        sample = (f"{sample_steps} DEM steps of the N={n} workload per benchmark step: the "
+                  f"reference's own kernels compiled for the host (oracle/_ref), one thread, "
+                  f"{sample_steps} instead of {INTERVAL} DEM steps per benchmark step to keep "
+                  f"the run within minutes")
+    else:
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        sample = (f"{sample_steps} DEM steps of the N={n} workload per benchmark step: the oracle "
+                  f"(a C restatement of the reference's FP64 step, pinned bit-exact against the "
+                  f"reference's own kernels built for the host), OpenMP on {cores} threads")
     cfg = workload_config(n)
-    cfg["dem_steps_per_step"] = args.ref_sample
+    cfg["dem_steps_per_step"] = sample_steps
     return {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -627,7 +651,7 @@ def run_reference(args):
         "config": cfg,
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
-                         "kind": "port", "sample": sample},
+                         "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -647,8 +671,9 @@ def main():
                          "the contact search reading neighbour cells staged in shared memory")
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--ref-sample", type=int, default=INTERVAL,
-                    help="DEM steps per benchmark step of the reference arm")
+    ap.add_argument("--ref-sample", type=int, default=0,
+                    help="DEM steps per benchmark step of the reference arm (0: %d with the "
+                         "reference's host build, %d with the oracle port)" % (REF_BUILD_SAMPLE, INTERVAL))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--darcy-steps", type=int, default=200,
                     help="fluid steps per arm of the Darcy leg (0 skips it)")

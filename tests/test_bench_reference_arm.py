@@ -4,7 +4,8 @@ The settled 100,000-sphere packing ships as a packaged fixture
 (sphere_b200/data, written by `python -m sphere_b200.prepack --pack` from the
 packing configs.settle_packing made on the GPU), so the dense-shear workload
 is the same bytes on every machine and `bench.py --impl reference` times the
-oracle without loading the engine library."""
+reference's own kernels built for the host (or the oracle where that build is
+absent) without loading the engine library."""
 import hashlib
 import os
 import subprocess
@@ -32,7 +33,8 @@ def test_reference_arm_never_loads_the_engine():
         "maps = open('/proc/self/maps').read()\n"
         "print('engine-module', 'sphere_b200.engine' in sys.modules)\n"
         "print('engine-library', 'libsphere_b200.so' in maps)\n"
-        "print('oracle-library', 'liboracle.so' in maps)\n"
+        "print('reference-library', 'libsphere_ref.so' in maps or 'liboracle.so' in maps)\n"
+        "print('kind', out['cpu_baseline']['kind'])\n"
         "print('config', out['config']['dem_steps_per_step'])\n" % ROOT)
     env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "4"))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT,
@@ -41,5 +43,7 @@ def test_reference_arm_never_loads_the_engine():
     lines = dict(line.split(" ", 1) for line in r.stdout.strip().splitlines() if " " in line)
     assert lines["engine-module"] == "False"
     assert lines["engine-library"] == "False"
-    assert lines["oracle-library"] == "True"
+    assert lines["reference-library"] == "True"
+    import oracle as O
+    assert lines["kind"] == ("reference" if O.ref_available() else "port")
     assert lines["config"] == "1"
