@@ -79,3 +79,23 @@ def test_mixed_step_from_reference_state_matches_fp64():
         e.set("delta_t", hist)
         e.step(1)
     assert rel(mix.get("force")[:, :3], ref2.get("force")[:, :3]) <= FORCE_TOL
+
+
+def test_staged_contact_kernel_mixed():
+    """The staged-cell contact kernel (step_kernel 3) in mixed precision:
+    the same contact sets as the list kernel and forces within the mixed
+    mode's bound of FP64 (FP32 arithmetic may contract differently in the
+    two kernels, so equality is not asked)."""
+    from sphere_b200.engine import Engine
+    d = dense_shear(43)
+    ref = Engine(d, precision="fp64")
+    lst = Engine(d, precision="mixed", step_kernel="stages")
+    stg = Engine(d, precision="mixed", step_kernel="stages_staged")
+    for e in (ref, lst, stg):
+        assert e.step(20) == 0
+    f_ref = ref.get("force")[:, :3]
+    assert numpy.array_equal(lst.get("contacts"), stg.get("contacts"))
+    assert rel(stg.get("force")[:, :3], f_ref) <= FORCE_TOL * 10
+    assert rel(lst.get("force")[:, :3], f_ref) <= FORCE_TOL * 10
+    for e in (ref, lst, stg):
+        e.close()
