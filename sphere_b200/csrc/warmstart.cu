@@ -56,16 +56,6 @@ struct ConvArgs {
     int *err;
 };
 
-__device__ __forceinline__ bool neighbour(const ConvArgs &a, unsigned c, int tap, size_t &nb)
-{
-    const int x = (int)(c % (unsigned)a.nx), y = (int)((c / (unsigned)a.nx) % (unsigned)a.ny);
-    const int z = (int)(c / ((unsigned)a.nx * (unsigned)a.ny));
-    const int xx = x + tap % 3 - 1, yy = y + (tap / 3) % 3 - 1, zz = z + tap / 9 - 1;
-    if (xx < 0 || xx >= a.nx || yy < 0 || yy >= a.ny || zz < 0 || zz >= a.nz) return false;
-    nb = (size_t)xx + (size_t)a.nx * ((size_t)yy + (size_t)a.ny * (size_t)zz);
-    return true;
-}
-
 // mode 0: out = ReLU(conv + bias) (BF16); mode 1: out channel 0 = conv +
 // bias (FP32); mode 2: out = conv * [relu_ref > 0] (BF16, no bias).
 //
@@ -97,18 +87,38 @@ __global__ void __launch_bounds__(128, 4) k_conv_tc(ConvArgs a)
     bool ok = true;
     const uint32_t aaddr = tc::smem_u32(sA), baddr = tc::smem_u32(sB);
     constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 16);
+    // this thread gathers the channel half h of tile rows r0 and r0 + 64:
+    // their grid coordinates once, then one offset per tap.  The eight lanes
+    // of a shared-memory store phase take eight consecutive rows (eight
+    // different bank groups of the no-swizzle layout).
+    const int h = (tid >> 3) & 1, r0 = ((tid >> 4) << 3) | (tid & 7);
+    int gx[2], gy[2], gz[2];
+    bool gv[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const unsigned c = c0 + (unsigned)(r0 + 64 * q);
+        gv[q] = c < a.ncells;
+        gx[q] = (int)(c % (unsigned)a.nx);
+        gy[q] = (int)((c / (unsigned)a.nx) % (unsigned)a.ny);
+        gz[q] = (int)(c / ((unsigned)a.nx * (unsigned)a.ny));
+    }
     for (int round = 0; round < kTaps / kRound; ++round) {
         // A: the tile's neighbour values per tap of this round, row = cell,
         // k = channel
-        for (int i = tid; i < kRound * 256; i += 128) {
-            const int tl = i >> 8, r = (i >> 1) & 127, h = i & 1;
+#pragma unroll
+        for (int tl = 0; tl < kRound; ++tl) {
             const int tap = round * kRound + tl;
-            const unsigned c = c0 + r;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            size_t nb;
-            if (c < a.ncells && neighbour(a, c, tap, nb))
-                v = *reinterpret_cast<const uint4 *>(a.in + nb * 16 + h * 8);
-            *reinterpret_cast<uint4 *>(sA + tl * 4096 + tc::kmajor_off(r, h * 8)) = v;
+            const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int xx = gx[q] + dx, yy = gy[q] + dy, zz = gz[q] + dz;
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (gv[q] && xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz) {
+                    const size_t nb = (size_t)xx + (size_t)a.nx * ((size_t)yy + (size_t)a.ny * (size_t)zz);
+                    v = *reinterpret_cast<const uint4 *>(a.in + nb * 16 + h * 8);
+                }
+                *reinterpret_cast<uint4 *>(sA + tl * 4096 + tc::kmajor_off((uint32_t)(r0 + 64 * q), h * 8)) = v;
+            }
         }
         tc::fence_smem_to_async();
         tc::fence_before_sync();
@@ -176,11 +186,13 @@ struct WgradArgs {
 
 // Weight and bias gradients of one layer over this block's range of cells,
 // in chunks of 64 cells (K = 4 slices of 16).  A holds the shifted inputs
-// transposed, rows (tap, in channel) in four M tiles of 128, columns =
-// cells: one thread takes 8 consecutive cells of one tap, loads their 16
-// channels and writes the 16 rows' 16-byte segments (a register transpose
-// instead of 2-byte shared-memory stores).  72 KB of shared memory keep
-// three blocks resident per SM.
+// transposed, columns = cells, in four M tiles of 128 rows: tile t holds
+// taps 8t..8t+7, row = in channel * 8 + tap % 8.  One thread takes 8
+// consecutive cells of one tap, loads their 16 channels and writes the 16
+// rows' 16-byte segments (a register transpose instead of 2-byte
+// shared-memory stores); consecutive lanes take consecutive taps, so the
+// eight lanes of a store phase write eight different bank groups.  72 KB of
+// shared memory keep three blocks resident per SM.
 __global__ void __launch_bounds__(128, 3) k_wgrad_tc(WgradArgs a)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -188,6 +200,7 @@ __global__ void __launch_bounds__(128, 3) k_wgrad_tc(WgradArgs a)
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base;
     __shared__ float bsum[kWChunk][17];
+    __shared__ int3 cxyz[kWChunk];
     const int tid = threadIdx.x, warp = tid >> 5;
     const unsigned cb = blockIdx.x * a.cells_per_block;
     const unsigned ce = min(cb + a.cells_per_block, a.ncells);
@@ -200,8 +213,6 @@ __global__ void __launch_bounds__(128, 3) k_wgrad_tc(WgradArgs a)
     for (unsigned i = tid; i < 16 * 4096 / 16; i += 128)
         reinterpret_cast<uint4 *>(sA)[i] = make_uint4(0u, 0u, 0u, 0u);
     float bacc = 0.0f;   // thread co < 16: bias gradient of channel co
-    ConvArgs geo;
-    geo.nx = a.nx; geo.ny = a.ny; geo.nz = a.nz; geo.ncells = a.ncells;
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -209,16 +220,28 @@ __global__ void __launch_bounds__(128, 3) k_wgrad_tc(WgradArgs a)
     bool ok = true;
     unsigned chunk = 0;
     for (unsigned base = cb; base < ce; base += kWChunk, ++chunk) {
-        // A: item = (tap, group of 8 cells)
-        for (int item = tid; item < kTaps * (kWChunk / 8); item += 128) {
-            const int tap = item / (kWChunk / 8), g = item % (kWChunk / 8);
+        // grid coordinates of the chunk's cells (x, y, z; x < 0: past the range)
+        if (tid < kWChunk) {
+            const unsigned c = base + (unsigned)tid;
+            cxyz[tid] = c < ce ? make_int3((int)(c % (unsigned)a.nx),
+                                           (int)((c / (unsigned)a.nx) % (unsigned)a.ny),
+                                           (int)(c / ((unsigned)a.nx * (unsigned)a.ny)))
+                               : make_int3(-2, 0, 0);
+        }
+        __syncthreads();
+        // A: item = (tap, group of 8 cells), taps fastest
+        for (int item = tid; item < 32 * (kWChunk / 8); item += 128) {
+            const int tap = item & 31, g = item >> 5;
+            if (tap >= kTaps) continue;
+            const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
             uint32_t w[8][8];   // [cell][channel pair]
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                const unsigned c = base + (unsigned)(g * 8 + j);
-                size_t nb;
+                const int3 p = cxyz[g * 8 + j];
+                const int xx = p.x + dx, yy = p.y + dy, zz = p.z + dz;
                 uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
-                if (c < ce && neighbour(geo, c, tap, nb)) {
+                if (p.x >= 0 && xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz) {
+                    const size_t nb = (size_t)xx + (size_t)a.nx * ((size_t)yy + (size_t)a.ny * (size_t)zz);
                     lo = *reinterpret_cast<const uint4 *>(a.x + nb * 16);
                     hi = *reinterpret_cast<const uint4 *>(a.x + nb * 16 + 8);
                 }
@@ -229,7 +252,7 @@ __global__ void __launch_bounds__(128, 3) k_wgrad_tc(WgradArgs a)
             const uint32_t kseg = (uint32_t)(g & 1) * 8;
 #pragma unroll
             for (int cp = 0; cp < 8; ++cp) {
-                const uint32_t row = (uint32_t)(tap & 7) * 16 + 2 * cp;
+                const uint32_t row = (uint32_t)(2 * cp) * 8 + (uint32_t)(tap & 7);
                 uint4 vlo, vhi;   // channel 2cp and 2cp+1 of the 8 cells
                 vlo.x = __byte_perm(w[0][cp], w[1][cp], 0x5410);
                 vlo.y = __byte_perm(w[2][cp], w[3][cp], 0x5410);
@@ -240,7 +263,7 @@ __global__ void __launch_bounds__(128, 3) k_wgrad_tc(WgradArgs a)
                 vhi.z = __byte_perm(w[4][cp], w[5][cp], 0x7632);
                 vhi.w = __byte_perm(w[6][cp], w[7][cp], 0x7632);
                 *reinterpret_cast<uint4 *>(tile + tc::kmajor_off(row, kseg)) = vlo;
-                *reinterpret_cast<uint4 *>(tile + tc::kmajor_off(row + 1, kseg)) = vhi;
+                *reinterpret_cast<uint4 *>(tile + tc::kmajor_off(row + 8, kseg)) = vhi;
             }
         }
         // B: slice kc holds rows = output channel, columns = cells
@@ -290,7 +313,8 @@ __global__ void __launch_bounds__(128, 3) k_wgrad_tc(WgradArgs a)
         uint32_t r[16];
         tc::tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(t * 16), r);
         tc::tmem_wait_ld();
-        const int m = t * 128 + warp * 32 + (tid & 31);
+        const int row = warp * 32 + (tid & 31);
+        const int m = (t * 8 + (row & 7)) * 16 + (row >> 3);   // tap * 16 + in channel
         for (int co = 0; co < 16; ++co) pw[(size_t)m * 16 + co] = (chunk > 0 && ok) ? __uint_as_float(r[co]) : 0.0f;
     }
     if (tid < 16) a.partial_b[(size_t)blockIdx.x * 16 + tid] = bacc;
