@@ -46,6 +46,9 @@ N_PARTICLES = 100000
 # capture of that kernel: 46.30 MB read + 3.15 MB written (ncu flushes the
 # caches before the launch)
 CONTACTS_TRAFFIC = 46.30e6 + 3.15e6
+# the same for one k_contacts_integrate<2,2> launch (contacts and
+# integration in one launch); None until captured
+FUSED_TRAFFIC = None
 SEED = 1
 
 
@@ -129,6 +132,12 @@ def workload_config(n):
     return {"workload": f"dense dry shear, N={n}, radii U(0.008,0.012) m, E=7e8 Pa, "
                         f"mu=0.5, sigma0=20 kPa, shear 1e-4 m/s, periodic x/y",
             "dem_steps_per_step": INTERVAL}
+
+
+def step_path_name(info):
+    """The step path the engine ran (sph_info.step_path)."""
+    return {1: "persistent", 2: "per-stage, contacts and integration in one launch"}.get(
+        int(info.step_path), "per-stage")
 
 
 def mean_contacts(eng, n):
@@ -266,12 +275,23 @@ def run_gpu(args):
     # es_dot, ev_dot, p write 24; es, ev read+write 32; per occupied slot
     # partner id 4 + tangential history 24, read and written (56)
     bytes_per_particle = 184.0 + 56.0 * zbar
+    kernel_name = "k_contacts (contact search + forces)"
+    traffic = CONTACTS_TRAFFIC if precision == "mixed" else None
+    if info.step_path == 2:
+        # contacts and integration in one launch: the integration's own
+        # fields (fixvel 8; angpos, acc0, angacc0, xyzsum read 96; pos, vel,
+        # angvel, angpos, acc, angacc, xyzsum written 168) come on top; its
+        # reads of force, torque, pos, vel and angvel are gone
+        bytes_per_particle += 272.0
+        kernel_name = "k_contacts_integrate (contact search + forces + integration)"
+        traffic = FUSED_TRAFFIC if precision == "mixed" else None
     contacts_bytes = n * bytes_per_particle
     achieved = contacts_bytes / (prof.contacts_ms * 1e-3) / 1e9
     # launches of this library's kernels in the timed region: per DEM step
     # k_resort (with the list rebuild), k_contacts, k_integrate (+2 for the
-    # shear-stress wall, +2 with bonds) on the per-stage path; one
-    # k_persistent per call on the fused path
+    # shear-stress wall, +2 with bonds) on the per-stage path, k_resort,
+    # k_contacts_integrate, k_walls_step with contacts and integration in one
+    # launch; one k_persistent per call on the persistent path
     if info.step_path == 1:
         timed_launches = args.steps
     else:
@@ -299,9 +319,9 @@ def run_gpu(args):
         "gpu_launches": timed_launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
-                     "traffic": CONTACTS_TRAFFIC if precision == "mixed" else None,
+                     "traffic": traffic,
                      "traffic_unit": "DRAM bytes per launch (ncu, cold caches)",
-                     "kernel": "k_contacts (contact search + forces)",
+                     "kernel": kernel_name,
                      "bytes_per_particle": bytes_per_particle,
                      "peak_source": peak_kind},
         "stage_ms_per_dem_step": {"resort": prof.resort_ms, "contacts": prof.contacts_ms,
@@ -309,7 +329,7 @@ def run_gpu(args):
                                   "step": prof.step_ms},
         "resorts": int(info.resorts),
         "shear_observables": shear,
-        "step_path": {"kernel": "persistent" if info.step_path == 1 else "per-stage",
+        "step_path": {"kernel": step_path_name(info),
                       "threads": int(info.step_threads), "grid": int(info.step_grid),
                       "autotuned": bool(info.tuned)},
         "clocks": clocks,
@@ -512,7 +532,7 @@ def settle_leg(args):
         "dem_steps": steps, "particle_steps_per_s": d.np * steps / (ms * 1e-3),
         "us_per_dem_step": 1e3 * ms / steps, "resorts": int(info.resorts),
         "mean_contacts_per_particle_at_end": zbar,
-        "step_path": "persistent" if info.step_path == 1 else "per-stage",
+        "step_path": step_path_name(info),
     }
 
 
@@ -553,7 +573,7 @@ def large_leg(args):
         "fp64_plain_particle_steps_per_s": fp64_rate,
         "mixed_over_fp64": n * interval * len(times) / step_s / fp64_rate,
         "mean_contacts_per_particle": zbar,
-        "step_path": "persistent" if info.step_path == 1 else "per-stage",
+        "step_path": step_path_name(info),
         "stage_ms_per_dem_step": {"resort": prof.resort_ms, "contacts": prof.contacts_ms,
                                   "bonds": prof.bonds_ms, "integrate": prof.integrate_ms,
                                   "step": prof.step_ms},
@@ -665,10 +685,11 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["faithful", "fp64", "mixed"])
     ap.add_argument("--step-kernel", default="auto",
-                    choices=["auto", "stages", "persistent", "stages_staged"],
+                    choices=["auto", "stages", "persistent", "stages_staged", "stages_fused"],
                     help="step path of the shear leg: automatic (autotuned), the per-stage "
-                         "kernels, the fused persistent kernel, or the per-stage kernels with "
-                         "the contact search reading neighbour cells staged in shared memory")
+                         "kernels, the fused persistent kernel, the per-stage kernels with "
+                         "the contact search reading neighbour cells staged in shared memory, "
+                         "or the per-stage kernels with contacts and integration in one launch")
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--ref-sample", type=int, default=0,

@@ -73,7 +73,11 @@ typedef struct sph_opts {
                              it does not apply: bonds, fluid, wmode 3), 3 per-stage
                              kernels with the contact search reading its partners
                              from the neighbour cells staged in shared memory
-                             (same results; slower on the measured workloads) */
+                             (same results; slower on the measured workloads),
+                             4 per-stage kernels with the contact search and the
+                             particle integration in one launch, integrating into
+                             a second buffer of x / vel / angvel (same results;
+                             error where it does not apply: bonds, fluid, wmode 3) */
     int darcy_exact_stop; /* 1: the Darcy Jacobi loop tests the residual at every
                              iteration and stops at the first that meets the
                              tolerance; 0 (default): the reference's test at
@@ -162,7 +166,8 @@ typedef struct sph_info {
     double time, time_total, dt, file_dt;
     uint32_t step_count;
     int64_t resorts;      /* re-sorts performed (steps where a particle changed cell) */
-    int32_t step_path;    /* 0 per-stage kernels, 1 fused persistent step */
+    int32_t step_path;    /* 0 per-stage kernels, 1 fused persistent step, 2 per-stage
+                             kernels with contacts and integration in one launch */
     int32_t step_threads; /* persistent path: threads per block chosen by the autotuner */
     int32_t step_grid;    /* persistent path: blocks of the launch */
     int32_t tuned;        /* 1 once the autotuner has run */

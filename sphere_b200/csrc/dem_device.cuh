@@ -872,4 +872,59 @@ __device__ __forceinline__ bool integrate_particle(const DevParams &P, const Dev
                             resort_flag, nl_flag);
 }
 
+// Copies sorted particle k's x / vel / angvel (and their FP32 copies) into
+// the other buffer of the ping-pong pair unchanged: a step that does not
+// integrate k still hands its state on to the next buffer.
+__device__ __forceinline__ void carry_particle(const DevState &S, unsigned k)
+{
+    S.x_nx[k] = S.x[k];
+    S.vel_nx[k] = S.vel[k];
+    S.angvel_nx[k] = S.angvel[k];
+    if (S.vel_f_nx) {
+        S.vel_f_nx[k] = S.vel_f[k];
+        S.angvel_f_nx[k] = S.angvel_f[k];
+    }
+}
+
+// The contact stage and the particle integration of one DEM step in one
+// launch, for dry boxes without bonds, fluid or a shear-stress wall (their
+// forces would have to join before the integration).  Thread k runs sorted
+// particle k's contact search and forces, writes them back, then integrates
+// it into the other buffer of the x / vel / angvel ping-pong pair
+// (S.x_nx, ...).  Every partner is read from the current buffer, which no
+// thread of this launch writes, so the step computes exactly what
+// k_contacts followed by k_integrate computes.  The cell and list flags of
+// the next step go to DevCtl::resort_next / nl_next (k_walls_step
+// publishes them after this launch); the wall reduction and the loop
+// counters follow in k_walls_step.  After a device error (raised by an
+// earlier step, or by this particle's contact search) the particle's state
+// is carried to the other buffer unchanged.
+template <int PREC, int MODEL>
+__global__ void __launch_bounds__(SPHB_CONTACT_B, SPHB_CONTACT_MINB)
+k_contacts_integrate(DevParams P, DevState S)
+{
+    extern __shared__ uint32_t srow[];   // blockDim * nc slot partners
+    DevCtl *ctl = S.ctl;
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.np) return;
+    if (ctl->err) {
+        carry_particle(S, k);
+        return;
+    }
+    StepClock clk;
+    clk.iter = ctl->iter;
+    clk.t_current = ctl->t_current;
+    clk.velocity_state = ctl->velocity_state;
+    clk.tau_eff_x = ctl->tau_eff_x;
+    ContactOut c;
+    if (!contact_particle<PREC, MODEL>(P, S, k, srow, blockDim.x, threadIdx.x, c)) {
+        carry_particle(S, k);
+        return;
+    }
+    contact_writeback(P, S, k, c);
+    integrate_particle(P, S, k, make_double4(c.F.x, c.F.y, c.F.z, 0.0f),
+                       make_double4(c.T.x, c.T.y, c.T.z, 0.0f), clk, S.x_nx, S.vel_nx,
+                       S.angvel_nx, S.vel_f_nx, S.angvel_f_nx, &ctl->resort_next, &ctl->nl_next);
+}
+
 }  // namespace sphb

@@ -43,6 +43,27 @@ cudaError_t launch_contacts_mixed(const DevParams &P, const DevState &S, cudaStr
     return cudaGetLastError();
 }
 
+cudaError_t launch_contacts_integrate_mixed(const DevParams &P, const DevState &S, cudaStream_t st)
+{
+    if (P.np == 0) return cudaSuccess;
+    const unsigned B = SPHB_CONTACT_B;
+    dim3 grid((P.np + B - 1) / B);
+    if (P.contactmodel == 2) {
+        size_t smem = (size_t)B * P.nc * sizeof(uint32_t);
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_contacts_integrate<2, 2>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)((size_t)B * 64 * sizeof(uint32_t)));
+            attr = true;
+        }
+        k_contacts_integrate<2, 2><<<grid, B, smem, st>>>(P, S);
+    } else {
+        k_contacts_integrate<2, 1><<<grid, B, 0, st>>>(P, S);
+    }
+    return cudaGetLastError();
+}
+
 int Engine::mixed_init() { return ST_OK; }
 
 }  // namespace sphb

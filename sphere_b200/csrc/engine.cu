@@ -143,7 +143,8 @@ int Engine::allocate_and_upload()
         S.angvel_f = dalloc<float4>(n);
         S.delta_t_f = dalloc<float4>(slots);
     }
-    if (persist_eligible()) {
+    // the other buffer of the x / vel / angvel pair for the fused step paths
+    if (fused_eligible() && step_kernel != 1 && step_kernel != 3) {
         S.x_nx = dalloc<double4>(n); S.vel_nx = dalloc<double4>(n); S.angvel_nx = dalloc<double4>(n);
         if (precision == SPH_PREC_MIXED) {
             S.vel_f_nx = dalloc<float4>(n);
@@ -293,12 +294,23 @@ cudaError_t Engine::enqueue_stage(int stage)
     switch (stage) {
     case 0: return launch_resort(P, S, S.perm_scratch, 0, stream, 1);
     case 1:
+        if (fused) {
+            if (precision == SPH_PREC_MIXED) return launch_contacts_integrate_mixed(P, S, stream);
+            return launch_contacts_integrate(P, S, prec, stream);
+        }
         if (precision == SPH_PREC_MIXED)
             return launch_contacts_mixed(P, S, stream, step_kernel == 3);
         return launch_contacts(P, S, prec, stream, step_kernel == 3);
     case 2: return launch_bonds(P, S, prec, bond_f, bond_t, stream);
     case 3: return enqueue_fluid();
-    case 4: return launch_integrate(P, S, stream);
+    case 4:
+        if (fused) {
+            // the step's integration went to the other buffer: it is current now
+            cudaError_t e = launch_walls_step(P, S, stream);
+            flip_view();
+            return e;
+        }
+        return launch_integrate(P, S, stream);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -356,13 +368,14 @@ int Engine::ensure_graph()
 {
     // kernels capture the state view by value: a graph made for the other
     // view (the persistent path flips views) is stale
-    if (graph_exec && graph_view != cur_view) {
+    if (graph_exec && (graph_view != cur_view || graph_fused != fused)) {
         cudaGraphExecDestroy(graph_exec);
         graph_exec = nullptr;
     }
     if (graph_exec || graph_steps <= 1 || graph_failed) return ST_OK;
     graph_view = cur_view;
-    graph_exec = capture_steps(graph_steps);
+    graph_fused = fused;
+    graph_exec = capture_steps(graph_len());
     if (!graph_exec) graph_failed = true;
     return ST_OK;
 }
@@ -373,6 +386,7 @@ cudaGraphExec_t Engine::capture_steps(int k)
 {
     cudaGraph_t g = nullptr;
     cudaGraphExec_t x = nullptr;
+    const int view0 = cur_view;   // fused steps flip the view while they are captured
     cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { cudaGetLastError(); return nullptr; }
     for (int i = 0; i < k && e == cudaSuccess; ++i) e = enqueue_step();
@@ -380,6 +394,8 @@ cudaGraphExec_t Engine::capture_steps(int k)
     if (e != cudaSuccess || e2 != cudaSuccess || !g) {
         if (g) cudaGraphDestroy(g);
         cudaGetLastError();
+        cur_view = view0;
+        S = S_view[cur_view];
         return nullptr;
     }
     e = cudaGraphInstantiate(&x, g, 0);
@@ -411,10 +427,11 @@ int Engine::step_stages(uint64_t n)
     }
     ensure_graph();
     uint64_t done = 0;
-    while (graph_exec && n - done >= (uint64_t)graph_steps) {
+    const uint64_t glen = (uint64_t)graph_len();
+    while (graph_exec && n - done >= glen) {
         cudaError_t e = cudaGraphLaunch(graph_exec, stream);
         if (e != cudaSuccess) return cuda_fail(e, "graph launch");
-        done += graph_steps;
+        done += glen;
     }
     for (; done < n; ++done) {
         cudaError_t e = enqueue_step();
@@ -831,7 +848,7 @@ static int open_common(std::unique_ptr<Engine> &eng, const sph_opts *opts)
     e.darcy_exact_stop = o.darcy_exact_stop ? 1 : 0;
     e.inject = (uint32_t)o.inject_timeout;
     e.outdir = o.output_dir ? o.output_dir : "output";
-    if (e.step_kernel < 0 || e.step_kernel > 3) return e.fail(sphb::ST_ARG, "unknown step_kernel");
+    if (e.step_kernel < 0 || e.step_kernel > 4) return e.fail(sphb::ST_ARG, "unknown step_kernel");
     if (e.precision != SPH_PREC_FAITHFUL && e.precision != SPH_PREC_FP64 &&
         e.precision != SPH_PREC_MIXED)
         return e.fail(sphb::ST_ARG, "unknown precision mode");
@@ -857,6 +874,10 @@ static int open_common(std::unique_ptr<Engine> &eng, const sph_opts *opts)
     if (e.step_kernel == 2 && !e.persist_eligible())
         return e.fail(sphb::ST_UNSUPPORTED, "the fused step kernel does not cover bonds, fluid or "
                                             "the shear-stress wall (wmode 3)");
+    if (e.step_kernel == 4 && !e.fused_eligible())
+        return e.fail(sphb::ST_UNSUPPORTED, "contacts and integration in one launch do not cover "
+                                            "bonds, fluid or the shear-stress wall (wmode 3)");
+    e.fused = e.step_kernel == 4;
     rc = e.allocate_and_upload();
     if (rc) return rc;
     rc = e.darcy_init();

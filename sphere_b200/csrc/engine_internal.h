@@ -36,7 +36,9 @@ public:
     int graph_steps = 64;
     int warm_start = 0;
     int warm_start_train = 2000;  // solves the warm-start network trains on
-    int step_kernel = 0;          // 0 automatic, 1 per-stage kernels, 2 persistent
+    int step_kernel = 0;          // 0 automatic, 1 per-stage kernels, 2 persistent,
+                                  // 3 per-stage with staged contacts, 4 per-stage with
+                                  // contacts and integration in one launch
     uint32_t inject = 0;          // SPH_INJECT_* mask (a test knob; 0 in normal use)
     std::string outdir = "output";
     std::string sid = "unnamed";
@@ -59,6 +61,7 @@ public:
 
     cudaGraphExec_t graph_exec = nullptr;
     int graph_view = -1;          // state view the graph was captured with
+    bool graph_fused = false;     // the graph holds fused per-stage steps
     bool graph_failed = false;
     bool warmed = false;
 
@@ -71,6 +74,11 @@ public:
     DevState S_view[2]{};         // S_view[v]: buffer view v (S is the current one)
     int cur_view = 0;
     bool persist_off = false;     // the autotuner found the per-stage kernels faster
+    // per-stage steps with the contact search and the particle integration
+    // in one launch (k_contacts_integrate into the other buffer of the
+    // x / vel / angvel pair, then k_walls_step); each step flips the view
+    bool fused = false;
+    int view_upload = 0;          // host source of the view copied to the persistent kernel
     FILE *convlog = nullptr;
     int jacobi_grid = 0;            // blocks of the cooperative Jacobi launch
     int darcy_exact_stop = 0;       // 1: stop at the first converged iteration
@@ -138,6 +146,12 @@ public:
 
     // mixed precision
     int mixed_init();
+
+    // fused per-stage step path
+    bool fused_eligible() const;
+    void set_fused(bool on);
+    void flip_view();
+    int graph_len() const;
 
     // fused persistent step path
     bool persist_eligible() const;

@@ -45,11 +45,46 @@ cudaError_t launch_refresh_f(const DevParams &P, const DevState &S, cudaStream_t
     return cudaGetLastError();
 }
 
+// Both fused step paths integrate inside the contact pass, so they cover
+// dry runs without bonds or the shear-stress wall: those forces would have
+// to join the contact forces before the integration.
+bool Engine::fused_eligible() const
+{
+    return !hs.fluid && hs.nb0 == 0 && !(hs.nw > 0 && hs.wmode[0] == 3) && hs.np > 0;
+}
+
 bool Engine::persist_eligible() const
 {
-    if (step_kernel == 1 || step_kernel == 3) return false;
-    // the fused step covers dry runs without bonds or the shear-stress wall
-    return !hs.fluid && hs.nb0 == 0 && !(hs.nw > 0 && hs.wmode[0] == 3) && hs.np > 0;
+    if (step_kernel != 0 && step_kernel != 2) return false;
+    return fused_eligible();
+}
+
+// Selects the per-stage step kernels: the contact and integration kernels
+// (on == false) or k_contacts_integrate + k_walls_step.  A graph of the
+// other kind is dropped, and the next step runs eagerly first (kernel
+// attributes are set outside any capture).
+void Engine::set_fused(bool on)
+{
+    if (on == fused) return;
+    fused = on;
+    warmed = false;
+    if (graph_exec) {
+        cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
+}
+
+void Engine::flip_view()
+{
+    cur_view ^= 1;
+    S = S_view[cur_view];
+}
+
+// Steps per captured graph: even on the fused per-stage path, so every
+// replay starts and ends on the view the graph was captured with.
+int Engine::graph_len() const
+{
+    return graph_steps + ((fused && (graph_steps & 1)) ? 1 : 0);
 }
 
 void Engine::make_views()
@@ -102,7 +137,7 @@ void *Engine::persist_ctl() const { return persist ? (void *)persist->pc : nullp
 
 void Engine::persist_describe(sph_info *info) const
 {
-    info->step_path = (persist && !persist_off) ? 1 : 0;
+    info->step_path = (persist && !persist_off) ? 1 : (fused ? 2 : 0);
     info->step_threads = persist ? kPersistShapes[persist->shape].threads : 0;
     info->step_grid = persist ? (int32_t)persist->grid : 0;
     info->tuned = persist ? (persist->tuned ? 1 : 0) : 0;
@@ -132,6 +167,10 @@ cudaError_t Engine::persist_launch(uint64_t n, int shape, unsigned grid)
     const int threads = kPersistShapes[shape].threads;
     cudaError_t e = cudaMemsetAsync(D.sync, 0, D.sync_bytes, stream);
     if (e != cudaSuccess) return e;
+    // the per-stage fused steps flip the view on the host
+    view_upload = cur_view;
+    e = cudaMemcpyAsync(&D.pc->view, &view_upload, sizeof(int), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
     BatchArgs A;
     A.boxes = D.table;
     A.nbox = 1;
@@ -152,7 +191,10 @@ int Engine::step_persistent(uint64_t n)
     PersistDev &D = *persist;
     uint64_t done = 0;
     const uint64_t trial = 8;
-    const int ncand = kNumPersistShapes + (step_kernel == 2 ? 0 : 1);
+    // candidates: every block shape of the persistent kernel, then (unless
+    // the persistent path was requested) the per-stage kernels and the
+    // per-stage kernels with contacts and integration in one launch
+    const int ncand = kNumPersistShapes + (step_kernel == 2 ? 0 : 2);
     if (!D.tuned && n >= trial * (uint64_t)(ncand + 2)) {
         cudaEvent_t a, b;
         cudaEventCreate(&a);
@@ -162,10 +204,15 @@ int Engine::step_persistent(uint64_t n)
         int rc = ST_OK;
         cudaGraphExec_t trial_graph = nullptr;
         for (int cand = 0; cand < ncand && rc == ST_OK; ++cand) {
-            const bool stages = cand == kNumPersistShapes;
+            const bool stages = cand >= kNumPersistShapes;
             unsigned g = stages ? 1 : persist_grid(cand);
             if (!g) continue;
             if (stages) {
+                set_fused(cand == kNumPersistShapes + 1);
+                if (trial_graph) {
+                    cudaGraphExecDestroy(trial_graph);
+                    trial_graph = nullptr;
+                }
                 // warm the per-stage path: the eager first step, then the
                 // trial steps as one graph (as they run in production; eager
                 // launches would time the host, not the kernels)
@@ -198,10 +245,12 @@ int Engine::step_persistent(uint64_t n)
         if (trial_graph) cudaGraphExecDestroy(trial_graph);
         if (rc) return rc;
         D.tuned = true;
-        if (best_cand == kNumPersistShapes) {
+        if (best_cand >= kNumPersistShapes) {
             persist_off = true;
+            set_fused(best_cand == kNumPersistShapes + 1);
             return step_stages(n - done);
         }
+        set_fused(false);
         D.shape = best_cand;
         D.grid = persist_grid(best_cand);
     }

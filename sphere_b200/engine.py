@@ -165,7 +165,7 @@ def lib() -> ctypes.CDLL:
     return L
 
 
-STEP_KERNEL = {"auto": 0, "stages": 1, "persistent": 2, "stages_staged": 3}
+STEP_KERNEL = {"auto": 0, "stages": 1, "persistent": 2, "stages_staged": 3, "stages_fused": 4}
 
 
 def make_opts(fluid=False, precision="faithful", integrator=3, capacity=32, device=-1,

@@ -60,11 +60,12 @@ def cases():
 
 @pytest.mark.parametrize("name,data", list(cases()), ids=[c[0] for c in cases()])
 @pytest.mark.parametrize("precision", ["faithful", "fp64"])
-@pytest.mark.parametrize("kernel", ["stages", "persistent", "stages_staged"])
+@pytest.mark.parametrize("kernel", ["stages", "persistent", "stages_staged", "stages_fused"])
 def test_step_parity(tmp_path, name, data, precision, kernel):
-    """Every step path -- the per-stage kernels, the fused persistent kernel
-    and the per-stage kernels with the contact search reading the neighbour
-    cells staged in shared memory -- against the oracle, bit for bit."""
+    """Every step path -- the per-stage kernels, the fused persistent kernel,
+    the per-stage kernels with the contact search reading the neighbour
+    cells staged in shared memory, and the per-stage kernels with contacts
+    and integration in one launch -- against the oracle, bit for bit."""
     from sphere_b200.engine import Engine
     path = tmp_path / f"{name}.bin"
     binfile.write_bin(data, path)
@@ -101,6 +102,31 @@ def test_persistent_autotuned_run(tmp_path, precision):
     eng.close()
 
 
+@pytest.mark.parametrize("precision", ["faithful", "fp64"])
+def test_autotuned_run_over_every_step_path(tmp_path, precision):
+    """The automatic choice with a call long enough for the autotuner: trial
+    steps on every block shape of the persistent kernel, on the per-stage
+    kernels and on the per-stage kernels with contacts and integration in
+    one launch (whose steps alternate the x / vel / angvel buffers), then the
+    winner -- the state must advance exactly like the oracle throughout."""
+    from sphere_b200.engine import Engine
+    d = dense(12, n=700)
+    configs.shear_setup(d, 0.05, 20e3)
+    d.w_x[0] -= 0.003
+    path = tmp_path / "auto.bin"
+    binfile.write_bin(d, path)
+    orc = O.Oracle(str(path), precision=precision)
+    eng = Engine(str(path), precision=precision, graph_steps=8)
+    for n in (90, 7, 16):
+        assert eng.step(n) == 0
+        assert orc.step(n) == 0, orc.error()
+        bad = compare(eng, orc)
+        assert not bad, bad
+    assert eng.info().tuned == 1
+    assert int(eng.get("iter")[0]) == 113
+    eng.close()
+
+
 def test_persistent_refuses_bonds(tmp_path):
     """The fused step does not cover bonds: asking for it is an error, the
     automatic choice falls back to the per-stage kernels."""
@@ -111,6 +137,8 @@ def test_persistent_refuses_bonds(tmp_path):
     binfile.write_bin(d, path)
     with pytest.raises(EngineError):
         Engine(str(path), step_kernel="persistent")
+    with pytest.raises(EngineError):
+        Engine(str(path), step_kernel="stages_fused")
     with Engine(str(path)) as eng:
         assert eng.step(2) == 0
 
@@ -128,11 +156,11 @@ def extra_cases():
 
 @pytest.mark.parametrize("name,data,integrator", list(extra_cases()),
                          ids=[c[0] for c in extra_cases()])
-@pytest.mark.parametrize("kernel", ["stages", "persistent"])
+@pytest.mark.parametrize("kernel", ["stages", "persistent", "stages_fused"])
 def test_step_parity_wall_modulation_and_ty2(tmp_path, name, data, integrator, kernel):
     """The sinusoidal normal stress of wall 0 (sigma0 + A sin(2 pi f t),
     src/integration.cuh:383-384) and the two-term Taylor integrator
-    (src/integration.cuh:192-220, 417-427) on both step paths, bit for bit."""
+    (src/integration.cuh:192-220, 417-427) on every step path, bit for bit."""
     from sphere_b200.engine import Engine
     path = tmp_path / f"{name}.bin"
     binfile.write_bin(data, path)
@@ -179,6 +207,8 @@ def test_step_parity_shear_stress_wall(tmp_path, precision):
     eng.close()
     with pytest.raises(EngineError):
         Engine(str(path), precision=precision, step_kernel="persistent")
+    with pytest.raises(EngineError):
+        Engine(str(path), precision=precision, step_kernel="stages_fused")
 
 
 def capillary_box(seed):
@@ -202,7 +232,7 @@ CAP_RTOL_X = 1e-12
 
 
 @pytest.mark.parametrize("precision", ["faithful", "fp64"])
-@pytest.mark.parametrize("kernel", ["stages", "persistent"])
+@pytest.mark.parametrize("kernel", ["stages", "persistent", "stages_fused"])
 def test_step_parity_capillary(tmp_path, precision, kernel):
     from sphere_b200.engine import Engine
     d = capillary_box(11)

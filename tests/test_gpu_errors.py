@@ -26,7 +26,7 @@ def test_capacity_overflow_is_reported():
     most = int((rows != d.np).sum(axis=1).max())
     probe.close()
     assert most >= 3
-    for kernel in ("stages", "persistent"):
+    for kernel in ("stages", "persistent", "stages_fused"):
         e = Engine(d, capacity=2, step_kernel=kernel)
         with pytest.raises(EngineError) as exc:
             e.step(5)

@@ -47,11 +47,15 @@ def test_single_step_force_error(seed):
     assert numpy.linalg.norm(t_mix - t_ref) / scale <= FORCE_TOL
 
 
-def test_force_error_stays_small_over_100_steps():
+@pytest.mark.parametrize("step_kernel", ["auto", "stages_fused"])
+def test_force_error_stays_small_over_100_steps(step_kernel):
+    """Over 100 sheared steps, on the automatic step path and on the
+    per-stage path with contacts and integration in one launch (whose mixed
+    integration rounds with FMA contraction, like the persistent kernel's)."""
     from sphere_b200.engine import Engine
     d = dense_shear(43)
     ref = Engine(d, precision="fp64")
-    mix = Engine(d, precision="mixed")
+    mix = Engine(d, precision="mixed", step_kernel=step_kernel)
     for _ in range(4):
         ref.step(25)
         mix.step(25)

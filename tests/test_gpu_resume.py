@@ -26,7 +26,7 @@ def shear_box(seed):
 
 
 @pytest.mark.parametrize("precision", ["faithful", "mixed"])
-@pytest.mark.parametrize("step_kernel", ["stages", "persistent"])
+@pytest.mark.parametrize("step_kernel", ["stages", "persistent", "stages_fused"])
 def test_resume_is_exact(tmp_path, precision, step_kernel):
     from sphere_b200.engine import Engine
     d = shear_box(71)
