@@ -5,6 +5,7 @@
 #pragma once
 
 #include "dem_state.h"
+#include "reduce_device.cuh"
 
 namespace sphb {
 
@@ -886,27 +887,78 @@ __device__ __forceinline__ void carry_particle(const DevState &S, unsigned k)
     }
 }
 
-// The contact stage and the particle integration of one DEM step in one
-// launch, for dry boxes without bonds, fluid or a shear-stress wall (their
-// forces would have to join before the integration).  Thread k runs sorted
-// particle k's contact search and forces, writes them back, then integrates
-// it into the other buffer of the x / vel / angvel ping-pong pair
-// (S.x_nx, ...).  Every partner is read from the current buffer, which no
-// thread of this launch writes, so the step computes exactly what
-// k_contacts followed by k_integrate computes.  The cell and list flags of
-// the next step go to DevCtl::resort_next / nl_next (k_walls_step
-// publishes them after this launch); the wall reduction and the loop
-// counters follow in k_walls_step.  After a device error (raised by an
-// earlier step, or by this particle's contact search) the particle's state
-// is carried to the other buffer unchanged.
-template <int PREC, int MODEL>
-__global__ void __launch_bounds__(SPHB_CONTACT_B, SPHB_CONTACT_MINB)
-k_contacts_integrate(DevParams P, DevState S)
+// The 256-element tree sum of the wall-0 forces of chunk j (ORIGINAL
+// indices [256 j, 256 j + 256)) in the reference's summation order
+// (src/integration.cuh:309-341: cache[e] += cache[e + i] for i = 128, 64,
+// ..., 1), formed by one warp: lane l holds e = l + 32 q, q = 0..7, so the
+// levels 128, 64 and 32 pair values within a lane and the levels 16..1 are
+// shuffles.  The result is valid in lane 0.
+__device__ __forceinline__ double warp_chunk_tree_sum(const double *in, unsigned np, unsigned j)
 {
-    extern __shared__ uint32_t srow[];   // blockDim * nc slot partners
+    const unsigned lane = threadIdx.x & 31u;
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const unsigned idx = (j << 8) + lane + 32u * q;
+        double t = 0.0f;
+        if (idx < np) t += __ldcg(in + idx);
+        v[q] = t;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] += v[q + 4];
+    v[0] += v[2];
+    v[1] += v[3];
+    v[0] += v[1];
+#pragma unroll
+    for (unsigned i = 16; i != 0; i /= 2) v[0] += __shfl_down_sync(0xffffffffu, v[0], i);
+    return v[0];
+}
+
+// The end of the step, by the warp that completed the last chunk: the
+// chunk partials added in chunk order (the reference's serial loop,
+// integration.cuh:67-68, 376-378; every lane forms the same sum), then in
+// lane 0 the wall update, the loop counters and the next step's flags.
+__device__ __forceinline__ void finish_step(const DevParams &P, const DevState &S)
+{
+    const unsigned lane = threadIdx.x & 31u;
     DevCtl *ctl = S.ctl;
-    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= P.np) return;
+    double wforce = 0.0;
+    if (P.nw > 0) {
+        const unsigned n = P.nblocks256;
+        for (unsigned base = 0; base < n; base += 32) {
+            const double v = base + lane < n ? __ldcg(S.partials + base + lane) : 0.0;
+            const unsigned cnt = min(32u, n - base);
+            for (unsigned i = 0; i < cnt; ++i) wforce += __shfl_sync(0xffffffffu, v, i);
+        }
+    }
+    if (lane != 0) return;
+    ctl->ticket = 0;
+    // every particle of the launch has arrived: its flags are final (read
+    // from L2: this SM's L1 may hold the line from the start of the launch)
+    if (__ldcg(&ctl->resort_next)) ctl->resort = 1;
+    // lists rebuilt at the start of this step are current unless a particle
+    // has since left its skin
+    ctl->nl_rebuild = __ldcg(&ctl->nl_next);
+    ctl->resort_next = 0;
+    ctl->nl_next = 0;
+    if (*(volatile int *)&ctl->err) return;
+    const long long iter = ctl->iter;
+    const double t_current = ctl->t_current;
+    walls_integrate(P, S, wforce, iter, t_current);
+    ctl->velocity_state = next_velocity_state(ctl->velocity_state, t_current);
+    ctl->t_current = t_current + P.dt;
+    ctl->iter = iter + 1;
+}
+
+// Contacts, forces and integration of sorted particle k (the particle work
+// of k_contacts_integrate).  After a device error (raised by an earlier
+// step, or by this particle's contact search) the particle's state is
+// carried to the other buffer unchanged.
+template <int PREC, int MODEL>
+__device__ __forceinline__ void contacts_integrate_particle(const DevParams &P, const DevState &S,
+                                                            unsigned k, uint32_t *srow)
+{
+    DevCtl *ctl = S.ctl;
     if (ctl->err) {
         carry_particle(S, k);
         return;
@@ -925,6 +977,65 @@ k_contacts_integrate(DevParams P, DevState S)
     integrate_particle(P, S, k, make_double4(c.F.x, c.F.y, c.F.z, 0.0f),
                        make_double4(c.T.x, c.T.y, c.T.z, 0.0f), clk, S.x_nx, S.vel_nx,
                        S.angvel_nx, S.vel_f_nx, S.angvel_f_nx, &ctl->resort_next, &ctl->nl_next);
+}
+
+// One whole DEM step after the re-sort check, in one launch, for dry boxes
+// without bonds, fluid or a shear-stress wall (their forces would have to
+// join before the integration).  Thread k runs sorted particle k's contact
+// search and forces, writes them back, then integrates it into the other
+// buffer of the x / vel / angvel ping-pong pair (S.x_nx, ...).  Every
+// partner is read from the current buffer, which no thread of this launch
+// writes, so the particles advance exactly as with k_contacts followed by
+// k_integrate.
+//
+// The wall reduction needs every particle's wall force, in ORIGINAL index
+// order: each particle counts itself into its 256-index chunk
+// (S.chunk_count) once its wall force is written; the warp whose particle
+// completes a chunk forms that chunk's tree sum (the reference's partial
+// of block j) and counts the chunk done (DevCtl::ticket); the warp that
+// completes the last chunk adds the partials in order, moves the walls,
+// advances the loop counters and publishes the cell / list flags the
+// integration raised (DevCtl::resort_next / nl_next).  By then every thread
+// has read the walls and the clock, so nothing it changes is still in use.
+template <int PREC, int MODEL>
+__global__ void __launch_bounds__(SPHB_CONTACT_B, SPHB_CONTACT_MINB)
+k_contacts_integrate(DevParams P, DevState S)
+{
+    extern __shared__ uint32_t srow[];   // blockDim * nc slot partners
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = k < P.np;
+    unsigned chunk = 0;
+    if (valid) {
+        chunk = S.orig_of[k] >> 8;
+        contacts_integrate_particle<PREC, MODEL>(P, S, k, srow);
+    }
+    // every lane of the warp reaches this point (no early return above)
+    bool completes = false;
+    if (valid) {
+        __threadfence();   // this particle's wall force before its count
+        const unsigned size = min(256u, P.np - (chunk << 8));
+        completes = atomicAdd(&S.chunk_count[chunk], 1u) == size - 1;
+    }
+    unsigned m = __ballot_sync(0xffffffffu, completes);
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        const unsigned j = __shfl_sync(0xffffffffu, chunk, src);
+        __threadfence();   // the chunk's wall forces, written by other threads
+        double part = 0.0;
+        if (P.nw > 0) part = warp_chunk_tree_sum(S.walls_force_pp, P.np, j);
+        int last = 0;
+        if ((threadIdx.x & 31u) == 0) {
+            if (P.nw > 0) S.partials[j] = part;
+            S.chunk_count[j] = 0;
+            __threadfence();
+            last = atomicAdd(&S.ctl->ticket, 1u) == P.nblocks256 - 1;
+        }
+        if (__shfl_sync(0xffffffffu, last, 0)) {
+            __threadfence();   // every chunk's partial and every particle's flags
+            finish_step(P, S);
+        }
+    }
 }
 
 }  // namespace sphb

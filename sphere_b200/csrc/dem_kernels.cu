@@ -228,48 +228,6 @@ __global__ void __launch_bounds__(256, SPHB_INTEGRATE_MINB) k_integrate(DevParam
     ctl->iter = clk.iter + 1;
 }
 
-// The rest of a DEM step whose particles k_contacts_integrate integrated:
-// the wall reduction and wall update exactly as k_integrate's (block j forms
-// the reference's partial sum j, the last block adds the partials in order,
-// moves the walls and advances the loop counters), and the re-sort / list
-// flags that integration raised, published for the next step's k_resort.
-// Launched with ceil(np / 256) blocks.
-__global__ void __launch_bounds__(256) k_walls_step(DevParams P, DevState S)
-{
-    __shared__ double cache[256];
-    __shared__ bool last;
-    DevCtl *ctl = S.ctl;
-    if (P.nw > 0 && P.np > 0) {
-        double s = chunk_tree_sum(S.walls_force_pp, P.np, blockIdx.x, cache);
-        if (threadIdx.x == 0) S.partials[blockIdx.x] = s;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    double wforce = (P.nw > 0 && P.np > 0) ? ordered_sum<256>(S.partials, P.nblocks256, cache) : 0.0;
-    if (threadIdx.x != 0) return;
-    ctl->ticket = 0;
-    // the contact launch finished before this one started: its flags are final
-    if (ctl->resort_next) ctl->resort = 1;
-    // lists rebuilt at the start of this step are current unless a particle
-    // has since left its skin
-    ctl->nl_rebuild = ctl->nl_next;
-    ctl->resort_next = 0;
-    ctl->nl_next = 0;
-    if (*(volatile int *)&ctl->err) return;
-    const long long iter = ctl->iter;
-    const double t_current = ctl->t_current;
-    walls_integrate(P, S, wforce, iter, t_current);
-    ctl->velocity_state = next_velocity_state(ctl->velocity_state, t_current);
-    ctl->t_current = t_current + P.dt;
-    ctl->iter = iter + 1;
-}
-
 // Cell hash of the current positions (first step, after sph_set).
 __global__ void k_hash(DevParams P, DevState S)
 {
@@ -368,12 +326,6 @@ cudaError_t launch_contacts_integrate(const DevParams &P, const DevState &S, int
         if (prec == 0) k_contacts_integrate<0, 1><<<grid, B, 0, st>>>(P, S);
         else k_contacts_integrate<1, 1><<<grid, B, 0, st>>>(P, S);
     }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_walls_step(const DevParams &P, const DevState &S, cudaStream_t st)
-{
-    k_walls_step<<<P.np > 0 ? P.nblocks256 : 1, 256, 0, st>>>(P, S);
     return cudaGetLastError();
 }
 
