@@ -289,13 +289,13 @@ def run_gpu(args):
     achieved = contacts_bytes / (prof.contacts_ms * 1e-3) / 1e9
     # launches of this library's kernels in the timed region: per DEM step
     # k_resort (with the list rebuild), k_contacts, k_integrate (+2 for the
-    # shear-stress wall, +2 with bonds) on the per-stage path; k_resort and
-    # k_contacts_integrate with contacts and integration in one launch; one
-    # k_persistent per call on the persistent path
+    # shear-stress wall, +2 with bonds) on the per-stage path; k_resort,
+    # k_contacts_integrate and k_walls_step with contacts and integration in
+    # one launch; one k_persistent per call on the persistent path
     if info.step_path == 1:
         timed_launches = args.steps
     elif info.step_path == 2:
-        timed_launches = 2 * INTERVAL * args.steps
+        timed_launches = 3 * INTERVAL * args.steps
     else:
         per_step = 3 + (2 if d.nw > 0 and d.wmode[0] == 3 else 0) + (2 if d.nb0 > 0 else 0)
         timed_launches = per_step * INTERVAL * args.steps
@@ -837,7 +837,7 @@ def run_distributed(args, rank, world):
     if rank == 0:
         per_step = 3 + (2 if d.nw > 0 and d.wmode[0] == 3 else 0)
         if info.step_path == 2:
-            per_step = 2
+            per_step = 3
         out = {
             "metric": "particle-steps/s", "value": comb["value"], "unit": "particle-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

@@ -914,27 +914,33 @@ __device__ __forceinline__ double warp_chunk_tree_sum(const double *in, unsigned
     return v[0];
 }
 
-// The end of the step, by the warp that completed the last chunk: the
-// chunk partials added in chunk order (the reference's serial loop,
-// integration.cuh:67-68, 376-378; every lane forms the same sum), then in
-// lane 0 the wall update, the loop counters and the next step's flags.
+// The end of a step whose particles k_contacts_integrate advanced, by one
+// warp once every chunk partial is written: the partials added in chunk
+// order (the reference's serial loop, integration.cuh:67-68, 376-378;
+// every lane forms the same sum), then in lane 0 the wall update, the loop
+// counters and the next step's flags.
 __device__ __forceinline__ void finish_step(const DevParams &P, const DevState &S)
 {
     const unsigned lane = threadIdx.x & 31u;
     DevCtl *ctl = S.ctl;
     double wforce = 0.0;
     if (P.nw > 0) {
+        // 32 partials per round, the next round's already in flight; past
+        // the last partial the lanes hold +0.0, which leaves the sum
+        // unchanged (it starts at +0.0, so it is never -0.0)
         const unsigned n = P.nblocks256;
+        double v = lane < n ? __ldcg(S.partials + lane) : 0.0;
         for (unsigned base = 0; base < n; base += 32) {
-            const double v = base + lane < n ? __ldcg(S.partials + base + lane) : 0.0;
-            const unsigned cnt = min(32u, n - base);
-            for (unsigned i = 0; i < cnt; ++i) wforce += __shfl_sync(0xffffffffu, v, i);
+            const unsigned nx = base + 32 + lane;
+            const double vn = nx < n ? __ldcg(S.partials + nx) : 0.0;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) wforce += __shfl_sync(0xffffffffu, v, i);
+            v = vn;
         }
     }
     if (lane != 0) return;
     ctl->ticket = 0;
-    // every particle of the launch has arrived: its flags are final (read
-    // from L2: this SM's L1 may hold the line from the start of the launch)
+    // the flags the integration raised in the contact launch
     if (__ldcg(&ctl->resort_next)) ctl->resort = 1;
     // lists rebuilt at the start of this step are current unless a particle
     // has since left its skin
@@ -979,63 +985,23 @@ __device__ __forceinline__ void contacts_integrate_particle(const DevParams &P, 
                        S.angvel_nx, S.vel_f_nx, S.angvel_f_nx, &ctl->resort_next, &ctl->nl_next);
 }
 
-// One whole DEM step after the re-sort check, in one launch, for dry boxes
-// without bonds, fluid or a shear-stress wall (their forces would have to
-// join before the integration).  Thread k runs sorted particle k's contact
-// search and forces, writes them back, then integrates it into the other
-// buffer of the x / vel / angvel ping-pong pair (S.x_nx, ...).  Every
-// partner is read from the current buffer, which no thread of this launch
-// writes, so the particles advance exactly as with k_contacts followed by
-// k_integrate.
-//
-// The wall reduction needs every particle's wall force, in ORIGINAL index
-// order: each particle counts itself into its 256-index chunk
-// (S.chunk_count) once its wall force is written; the warp whose particle
-// completes a chunk forms that chunk's tree sum (the reference's partial
-// of block j) and counts the chunk done (DevCtl::ticket); the warp that
-// completes the last chunk adds the partials in order, moves the walls,
-// advances the loop counters and publishes the cell / list flags the
-// integration raised (DevCtl::resort_next / nl_next).  By then every thread
-// has read the walls and the clock, so nothing it changes is still in use.
+// The contact stage and the particle integration of one DEM step in one
+// launch, for dry boxes without bonds, fluid or a shear-stress wall (their
+// forces would have to join before the integration).  Thread k runs sorted
+// particle k's contact search and forces, writes them back, then integrates
+// it into the other buffer of the x / vel / angvel ping-pong pair
+// (S.x_nx, ...).  Every partner is read from the current buffer, which no
+// thread of this launch writes, so the particles advance exactly as with
+// k_contacts followed by k_integrate.  The cell and list flags of the next
+// step go to DevCtl::resort_next / nl_next; the wall reduction, the wall
+// update and the loop counters follow in k_walls_step.
 template <int PREC, int MODEL>
 __global__ void __launch_bounds__(SPHB_CONTACT_B, SPHB_CONTACT_MINB)
 k_contacts_integrate(DevParams P, DevState S)
 {
     extern __shared__ uint32_t srow[];   // blockDim * nc slot partners
     const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = k < P.np;
-    unsigned chunk = 0;
-    if (valid) {
-        chunk = S.orig_of[k] >> 8;
-        contacts_integrate_particle<PREC, MODEL>(P, S, k, srow);
-    }
-    // every lane of the warp reaches this point (no early return above)
-    bool completes = false;
-    if (valid) {
-        __threadfence();   // this particle's wall force before its count
-        const unsigned size = min(256u, P.np - (chunk << 8));
-        completes = atomicAdd(&S.chunk_count[chunk], 1u) == size - 1;
-    }
-    unsigned m = __ballot_sync(0xffffffffu, completes);
-    while (m) {
-        const int src = __ffs(m) - 1;
-        m &= m - 1;
-        const unsigned j = __shfl_sync(0xffffffffu, chunk, src);
-        __threadfence();   // the chunk's wall forces, written by other threads
-        double part = 0.0;
-        if (P.nw > 0) part = warp_chunk_tree_sum(S.walls_force_pp, P.np, j);
-        int last = 0;
-        if ((threadIdx.x & 31u) == 0) {
-            if (P.nw > 0) S.partials[j] = part;
-            S.chunk_count[j] = 0;
-            __threadfence();
-            last = atomicAdd(&S.ctl->ticket, 1u) == P.nblocks256 - 1;
-        }
-        if (__shfl_sync(0xffffffffu, last, 0)) {
-            __threadfence();   // every chunk's partial and every particle's flags
-            finish_step(P, S);
-        }
-    }
+    if (k < P.np) contacts_integrate_particle<PREC, MODEL>(P, S, k, srow);
 }
 
 }  // namespace sphb

@@ -228,6 +228,36 @@ __global__ void __launch_bounds__(256, SPHB_INTEGRATE_MINB) k_integrate(DevParam
     ctl->iter = clk.iter + 1;
 }
 
+// The rest of a DEM step whose particles k_contacts_integrate advanced: the
+// wall reduction and wall update of k_integrate in the same arithmetic.
+// Each warp forms the tree sums of chunks w, w + warps, ... (chunk j: the
+// reference's partial of block j, warp_chunk_tree_sum); the block that
+// finishes last adds the partials in chunk order, moves the walls, advances
+// the loop counters and publishes the cell / list flags of the next step
+// (finish_step).  Launched with ceil(chunks / 8) blocks of 256 threads.
+__global__ void __launch_bounds__(256) k_walls_step(DevParams P, DevState S)
+{
+    __shared__ bool last;
+    DevCtl *ctl = S.ctl;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned nwarps = gridDim.x * (blockDim.x >> 5);
+    if (P.nw > 0 && P.np > 0)
+        for (unsigned j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < P.nblocks256;
+             j += nwarps) {
+            const double part = warp_chunk_tree_sum(S.walls_force_pp, P.np, j);
+            if (lane == 0) S.partials[j] = part;
+        }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x >= 32) return;
+    __threadfence();
+    finish_step(P, S);
+}
+
 // Cell hash of the current positions (first step, after sph_set).
 __global__ void k_hash(DevParams P, DevState S)
 {
@@ -326,6 +356,13 @@ cudaError_t launch_contacts_integrate(const DevParams &P, const DevState &S, int
         if (prec == 0) k_contacts_integrate<0, 1><<<grid, B, 0, st>>>(P, S);
         else k_contacts_integrate<1, 1><<<grid, B, 0, st>>>(P, S);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_walls_step(const DevParams &P, const DevState &S, cudaStream_t st)
+{
+    const unsigned chunks = P.np > 0 ? P.nblocks256 : 1;
+    k_walls_step<<<blocks_for(chunks, 8), 256, 0, st>>>(P, S);
     return cudaGetLastError();
 }
 

@@ -20,13 +20,16 @@ cudaError_t launch_contacts_mixed(const DevParams &P, const DevState &S, cudaStr
 // Shared memory of the staged contact kernel: bytes per block and the
 // staging capacity (particles) for nc slots per particle.
 void staged_contact_shape(unsigned nc, size_t per_particle, size_t &smem, unsigned &cap);
-// Contacts, particle integration, wall reduction and wall update of one
-// step in one launch (k_contacts_integrate): reads the current buffers of
-// S, integrates into S.x_nx / vel_nx / angvel_nx (and the FP32 copies).
-// Only for dry boxes without bonds or a shear-stress wall.
+// Contacts and particle integration of one step in one launch
+// (k_contacts_integrate): reads the current buffers of S, integrates into
+// S.x_nx / vel_nx / angvel_nx (and the FP32 copies).  Only for dry boxes
+// without bonds or a shear-stress wall; launch_walls_step completes the step.
 cudaError_t launch_contacts_integrate(const DevParams &P, const DevState &S, int prec,
                                       cudaStream_t st);
 cudaError_t launch_contacts_integrate_mixed(const DevParams &P, const DevState &S, cudaStream_t st);
+// wall reduction, wall update, loop counters and the next step's flags after
+// launch_contacts_integrate
+cudaError_t launch_walls_step(const DevParams &P, const DevState &S, cudaStream_t st);
 cudaError_t launch_bonds(const DevParams &P, const DevState &S, int prec, double4 *bond_f,
                          double4 *bond_t, cudaStream_t st);
 // shear-stress reduction (wmode 3), then one kernel: integration, wall

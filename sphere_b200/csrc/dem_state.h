@@ -49,8 +49,6 @@ struct DevState {
     double *walls_force_pp;   // nw * np, ORIGINAL order (reduced like the reference)
     double *tau_pp;           // np, ORIGINAL order
     double *partials;         // nblocks256
-    uint32_t *chunk_count;    // nblocks256: particles of each 256-index chunk done this step
-                              // (k_contacts_integrate; zero between its launches)
     double *tau_partials;     // nblocks256
 
     // bonds (original particle indices)

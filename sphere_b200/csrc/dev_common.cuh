@@ -69,8 +69,8 @@ struct DevCtl {
     int nl_rebuild;            // 1: rebuild the neighbour lists before contacts
     long long nl_builds;       // neighbour-list builds performed
     // flags raised by an integration that runs inside the contact launch
-    // (k_contacts_integrate); its last warp moves them into resort /
-    // nl_rebuild once every particle of the launch is done
+    // (k_contacts_integrate); k_walls_step moves them into resort /
+    // nl_rebuild once that launch has finished
     int resort_next;
     int nl_next;
 };

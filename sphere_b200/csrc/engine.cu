@@ -150,7 +150,6 @@ int Engine::allocate_and_upload()
             S.vel_f_nx = dalloc<float4>(n);
             S.angvel_f_nx = dalloc<float4>(n);
         }
-        S.chunk_count = dalloc<uint32_t>(P.nblocks256);
         if (!S.x_nx || !S.vel_nx || !S.angvel_nx) return fail(ST_CUDA, "device allocation failed");
     }
     S.nl = dalloc<uint32_t>(n * (size_t)nlmax);
@@ -307,8 +306,9 @@ cudaError_t Engine::enqueue_stage(int stage)
     case 4:
         if (fused) {
             // the step's integration went to the other buffer: it is current now
+            cudaError_t e = launch_walls_step(P, S, stream);
             flip_view();
-            return cudaSuccess;
+            return e;
         }
         return launch_integrate(P, S, stream);
     default: return cudaErrorInvalidValue;
