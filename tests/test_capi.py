@@ -72,3 +72,20 @@ def test_open_refuses_a_mismatched_struct_size(tmp_path):
                       ctypes.cast(ctypes.byref(short), ctypes.POINTER(engine.SphOpts)), ctypes.byref(h))
     assert rc == -8 and not h.value
     assert b"struct_size" in lib.sph_open_error()
+
+
+def test_open_refuses_an_unknown_step_kernel(tmp_path):
+    """step_kernel is checked before the device is touched: 0-4 are the
+    automatic choice and the four step paths, anything else is an argument
+    error."""
+    from sphere_b200 import binfile, configs
+    assert engine.STEP_KERNEL == {"auto": 0, "stages": 1, "persistent": 2, "stages_staged": 3,
+                                  "stages_fused": 4}
+    path = tmp_path / "two.bin"
+    binfile.write_bin(configs.two_particle(z=(2.0, 6.0), vel0=0.0), path)
+    lib = engine.lib()
+    opts = engine.make_opts(step_kernel=5)
+    h = ctypes.c_void_p()
+    rc = lib.sph_open(str(path).encode(), ctypes.byref(opts), ctypes.byref(h))
+    assert rc == -8 and not h.value
+    assert b"step_kernel" in lib.sph_open_error()
