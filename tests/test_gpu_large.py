@@ -77,3 +77,23 @@ def test_mixed_force_error():
     a, b = out["mixed"], out["fp64"]
     err = float(numpy.linalg.norm(a - b) / numpy.linalg.norm(b))
     assert err <= 1e-5, err
+
+
+def test_step_paths_agree_on_the_shear_benchmark():
+    """The benchmark box itself (1e5 spheres, dense shear, faithful FP64):
+    300 DEM steps on the per-stage kernels and on the per-stage kernels with
+    contacts and integration in one launch (the step path the autotuner
+    picks there) end in bit-identical states, resorts and list rebuilds
+    included; the oracle pins the per-stage kernels on the smaller cases."""
+    from sphere_b200.engine import Engine
+    d = configs.shear_benchmark(n=100_000, seed=1)
+    names = ("x", "vel", "angvel", "angpos", "force", "torque", "acc", "angacc", "xyzsum",
+             "es", "ev", "p", "index", "contacts", "delta_t", "walls_nx", "walls_mvfd", "iter")
+    states = []
+    for kernel in ("stages", "stages_fused"):
+        with Engine(d, precision="faithful", graph_steps=50, step_kernel=kernel) as e:
+            assert e.step(300) == 0
+            states.append({f: e.get(f) for f in names})
+            assert e.info().resorts > 0
+    bad = [f for f in names if not numpy.array_equal(bits(states[0][f]), bits(states[1][f]))]
+    assert not bad, bad
