@@ -925,7 +925,7 @@ __device__ __forceinline__ void finish_step(const DevParams &P, const DevState &
     DevCtl *ctl = S.ctl;
     double wforce = 0.0;
     if (P.nw > 0) {
-        // 32 partials per round, the next round's already in flight; past
+        // 32 partials per pass, the next 32 already in flight; past
         // the last partial the lanes hold +0.0, which leaves the sum
         // unchanged (it starts at +0.0, so it is never -0.0)
         const unsigned n = P.nblocks256;
