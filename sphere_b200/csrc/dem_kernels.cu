@@ -230,30 +230,32 @@ __global__ void __launch_bounds__(256, SPHB_INTEGRATE_MINB) k_integrate(DevParam
 
 // The rest of a DEM step whose particles k_contacts_integrate advanced: the
 // wall reduction and wall update of k_integrate in the same arithmetic.
-// Each warp forms the tree sums of chunks w, w + warps, ... (chunk j: the
-// reference's partial of block j, warp_chunk_tree_sum); the block that
-// finishes last adds the partials in chunk order, moves the walls, advances
-// the loop counters and publishes the cell / list flags of the next step
-// (finish_step).  Launched with ceil(chunks / 8) blocks of 256 threads.
-__global__ void __launch_bounds__(256) k_walls_step(DevParams P, DevState S)
+// Warp j forms the tree sum of chunk j (the reference's partial of block j,
+// warp_chunk_tree_sum) and counts itself done (DevCtl::ticket); the warp
+// that counts last adds the partials in chunk order, moves the walls,
+// advances the loop counters and publishes the cell / list flags of the next
+// step (finish_step).  One warp per 256-index chunk, SPHB_WALLS_WARPS warps
+// per block, no block barrier.
+#ifndef SPHB_WALLS_WARPS
+#define SPHB_WALLS_WARPS 8
+#endif
+__global__ void __launch_bounds__(32 * SPHB_WALLS_WARPS) k_walls_step(DevParams P, DevState S)
 {
-    __shared__ bool last;
     DevCtl *ctl = S.ctl;
     const unsigned lane = threadIdx.x & 31u;
-    const unsigned nwarps = gridDim.x * (blockDim.x >> 5);
-    if (P.nw > 0 && P.np > 0)
-        for (unsigned j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < P.nblocks256;
-             j += nwarps) {
-            const double part = warp_chunk_tree_sum(S.walls_force_pp, P.np, j);
-            if (lane == 0) S.partials[j] = part;
-        }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
+    const unsigned j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const unsigned nchunks = P.np > 0 ? P.nblocks256 : 1;
+    if (j >= nchunks) return;   // whole warps
+    if (P.nw > 0 && P.np > 0) {
+        const double part = warp_chunk_tree_sum(S.walls_force_pp, P.np, j);
+        if (lane == 0) S.partials[j] = part;
     }
-    __syncthreads();
-    if (!last || threadIdx.x >= 32) return;
+    int last = 0;
+    if (lane == 0) {
+        __threadfence();
+        last = atomicAdd(&ctl->ticket, 1u) == nchunks - 1;
+    }
+    if (!__shfl_sync(0xffffffffu, last, 0)) return;
     __threadfence();
     finish_step(P, S);
 }
@@ -362,7 +364,7 @@ cudaError_t launch_contacts_integrate(const DevParams &P, const DevState &S, int
 cudaError_t launch_walls_step(const DevParams &P, const DevState &S, cudaStream_t st)
 {
     const unsigned chunks = P.np > 0 ? P.nblocks256 : 1;
-    k_walls_step<<<blocks_for(chunks, 8), 256, 0, st>>>(P, S);
+    k_walls_step<<<blocks_for(chunks, SPHB_WALLS_WARPS), 32 * SPHB_WALLS_WARPS, 0, st>>>(P, S);
     return cudaGetLastError();
 }
 
