@@ -274,6 +274,35 @@ __global__ void k_hash(DevParams P, DevState S)
     S.cell_new[k] = ((unsigned)iz * P.num[1]) * P.num[0] + (unsigned)iy * P.num[0] + (unsigned)ix;
 }
 
+// New positions (and radii) from the host, in ORIGINAL order, into the
+// sorted storage.  Each particle's cell is hashed (src/sorting.cuh:7-51) and
+// DevCtl::resort raised when it changed, DevCtl::nl_rebuild when the
+// particle left 0.45 skin of its position at the list build or its radius
+// changed -- the conditions under which the integration raises them -- so
+// the next step's k_resort sorts and rebuilds exactly when a forced sort
+// would have changed something (a stable sort of unchanged cells is the
+// identity).
+__global__ void k_set_positions(DevParams P, DevState S, const double4 *src)
+{
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.np) return;
+    const unsigned o = S.orig_of[k];
+    const double4 xo = S.x[k], xn = src[o];
+    int ix, iy, iz;
+    if (!cell_coord(P, xn.x, 0, ix) || !cell_coord(P, xn.y, 1, iy) || !cell_coord(P, xn.z, 2, iz)) {
+        raise_err(S.ctl, DERR_OUTSIDE, (int)o);
+        return;
+    }
+    const unsigned c = ((unsigned)iz * P.num[1]) * P.num[0] + (unsigned)iy * P.num[0] + (unsigned)ix;
+    S.x[k] = xn;
+    S.cell_new[k] = c;
+    if (c != S.cell_of[k]) S.ctl->resort = 1;
+    const float4 xr = S.x_ref[k];
+    const double ddx = xn.x - (double)xr.x, ddy = xn.y - (double)xr.y, ddz = xn.z - (double)xr.z;
+    const double lim = 0.45 * P.skin;
+    if (xn.w != xo.w || ddx * ddx + ddy * ddy + ddz * ddz > lim * lim) S.ctl->nl_rebuild = 1;
+}
+
 // ---------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------
@@ -394,6 +423,14 @@ cudaError_t launch_occ_from_rows(const DevParams &P, const DevState &S, cudaStre
 {
     if (P.np == 0) return cudaSuccess;
     k_occ_from_rows<<<blocks_for(P.np, 256), 256, 0, st>>>(P, S);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_positions(const DevParams &P, const DevState &S, const double4 *src,
+                                 cudaStream_t st)
+{
+    if (P.np == 0) return cudaSuccess;
+    k_set_positions<<<blocks_for(P.np, 256), 256, 0, st>>>(P, S, src);
     return cudaGetLastError();
 }
 

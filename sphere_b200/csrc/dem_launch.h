@@ -37,6 +37,11 @@ cudaError_t launch_bonds(const DevParams &P, const DevState &S, int prec, double
 cudaError_t launch_integrate(const DevParams &P, const DevState &S, cudaStream_t st);
 cudaError_t launch_occ_from_rows(const DevParams &P, const DevState &S, cudaStream_t st);
 cudaError_t launch_hash(const DevParams &P, const DevState &S, cudaStream_t st);
+// positions from the host (ORIGINAL order, device memory) into the sorted
+// storage, raising the re-sort and list flags where a particle changed cell,
+// left its list skin or changed radius
+cudaError_t launch_set_positions(const DevParams &P, const DevState &S, const double4 *src,
+                                 cudaStream_t st);
 // force = 1 sorts unconditionally; otherwise only when DevCtl::resort is
 // set.  with_nl = 1 also rebuilds the neighbour lists in the same launch
 // when they are stale (DevCtl::nl_rebuild) or the sort ran.

@@ -600,12 +600,10 @@ int Engine::set(int f, const void *src, size_t bytes)
     cudaError_t e = cudaSuccess;
     if (double4 *dst = sorted_vec(f)) {
         e = cudaMemcpyAsync(tmp, src, n * 32, cudaMemcpyHostToDevice, stream);
-        if (e == cudaSuccess) e = launch_sort_into(tmp, dst, S.orig_of, n, 32, stream);
-        if (f == SPH_F_X && e == cudaSuccess) {
-            // positions changed: re-hash and re-sort before the next step
-            e = launch_hash(P, S, stream);
-            if (e == cudaSuccess) e = launch_resort(P, S, S.perm_scratch, 1, stream);
-        }
+        // positions: the next step re-sorts and rebuilds the lists where
+        // they changed (k_set_positions raises the flags)
+        if (e == cudaSuccess && f == SPH_F_X) e = launch_set_positions(P, S, (const double4 *)tmp, stream);
+        else if (e == cudaSuccess) e = launch_sort_into(tmp, dst, S.orig_of, n, 32, stream);
     } else if (double *dst = sorted_scalar(f)) {
         e = cudaMemcpyAsync(tmp, src, n * 8, cudaMemcpyHostToDevice, stream);
         if (e == cudaSuccess) e = launch_sort_into(tmp, dst, S.orig_of, n, 8, stream);
@@ -664,14 +662,10 @@ int Engine::set(int f, const void *src, size_t bytes)
         default: return fail(ST_ARG, "field is read-only");
         }
     }
-    if (e == cudaSuccess) {
-        static const int one = 1;
-        e = cudaMemcpyAsync(&S.ctl->nl_rebuild, &one, sizeof one, cudaMemcpyHostToDevice, stream);
-    }
-    if (e == cudaSuccess) e = launch_refresh_f(P, S, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    // the FP32 velocity copies of the mixed mode follow the FP64 velocities
+    if (e == cudaSuccess && (f == SPH_F_VEL || f == SPH_F_ANGVEL)) e = launch_refresh_f(P, S, stream);
     if (e != cudaSuccess) return cuda_fail(e, "set");
-    return poll_errors("set");
+    return poll_errors("set");   // waits for the copies out of the caller's buffer
 }
 
 int Engine::download_state()
