@@ -224,7 +224,11 @@ int64_t sph_field_bytes(sph_engine *e, sph_field f);
 /* Copies a field to host memory (synchronises the engine's stream). */
 int sph_get(sph_engine *e, sph_field f, void *dst, size_t bytes);
 
-/* Overwrites a field from host memory (positions, velocities, ...). */
+/* Overwrites a field from host memory (positions, velocities, ...);
+ * returns once the source buffer has been read.  New positions take effect
+ * at the next step, which re-sorts and rebuilds the neighbour lists where a
+ * particle changed cell, left its list skin or changed radius; a position
+ * outside the grid is reported here (SPH_ERR_OUTSIDE). */
 int sph_set(sph_engine *e, sph_field f, const void *src, size_t bytes);
 
 /* Writes the current state as a .bin file (src/file_io.cpp:420-731). */
