@@ -47,3 +47,15 @@ def test_reference_arm_never_loads_the_engine():
     import oracle as O
     assert lines["kind"] == ("reference" if O.ref_available() else "port")
     assert lines["config"] == "1"
+
+
+def test_step_path_names():
+    """The benchmark line names the step path the engine reports
+    (sph_info.step_path)."""
+    import types
+    sys.path.insert(0, ROOT)
+    import bench
+    name = lambda p: bench.step_path_name(types.SimpleNamespace(step_path=p))  # noqa: E731
+    assert name(0) == "per-stage"
+    assert name(1) == "persistent"
+    assert name(2) == "per-stage, contacts and integration in one launch"
